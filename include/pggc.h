@@ -1,0 +1,158 @@
+/*
+ * pggc.h -- C ABI of the B200-native PGGC clustering hot path.
+ *
+ * The reference exposes this path as C++ templates over Kokkos types; every
+ * entry point below replaces one of them with plain pointers and sizes (no
+ * Kokkos, no torch types).  Citations are to the reference project.
+ *
+ * Conventions
+ *   - Every call returns pggc_status; on failure pggc_last_error() returns a
+ *     thread-local message.  PGGC_ERR_DEVICE means a device-side bounded loop
+ *     (hash probe, pointer chase) gave up; the context stays usable.
+ *   - mem_kind says where caller arrays live: PGGC_MEM_HOST (pageable or
+ *     pinned host memory, copied in/out inside the call) or PGGC_MEM_DEVICE
+ *     (device pointers on the context's device).
+ *   - Weight kinds: PGGC_W_UNIFORM (unit weights, `weights` ignored),
+ *     PGGC_W_INT32 (int32 weights), PGGC_W_FLOAT32 (float32 weights).
+ *     Vertex weights / cluster volumes ("V" arrays) are int64 for the first two
+ *     and float64 for PGGC_W_FLOAT32.
+ *   - Graphs are symmetric CSR: int64 row offsets (n+1), int32 columns (nnz),
+ *     no self-loops, no duplicate edges.
+ *   - Calls on one context are serialised on the context's CUDA stream and
+ *     return after the work is complete.
+ */
+#ifndef PGGC_H
+#define PGGC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pggc_status {
+    PGGC_OK = 0,
+    PGGC_ERR_INVALID = 1,  /* bad argument or unsupported input            */
+    PGGC_ERR_CUDA = 2,     /* CUDA runtime error (message has the details)  */
+    PGGC_ERR_DEVICE = 3,   /* device-side bounded loop gave up              */
+    PGGC_ERR_INTERNAL = 4
+} pggc_status;
+
+enum { PGGC_W_UNIFORM = 0, PGGC_W_INT32 = 1, PGGC_W_FLOAT32 = 2 };
+/* app/io/parse_args.cpp:10-16 objective names: Mod, WMod, CPM, NLCC, LCC */
+enum { PGGC_OBJ_MOD = 0, PGGC_OBJ_WMOD = 1, PGGC_OBJ_CPM = 2, PGGC_OBJ_NLCC = 3, PGGC_OBJ_LCC = 4 };
+enum { PGGC_MEM_HOST = 0, PGGC_MEM_DEVICE = 1 };
+/* app/CMakeLists.txt:3-7: plouvain, pleiden, pleiden+ */
+enum { PGGC_METHOD_LOUVAIN = 0, PGGC_METHOD_LEIDEN = 1, PGGC_METHOD_LEIDEN_PLUS = 2 };
+
+typedef struct pggc_context pggc_context;           /* interface/memory_store.hpp:12-91   */
+typedef struct pggc_graph pggc_graph;               /* interface/weighted_graph.h:10-19   */
+typedef struct pggc_cluster_data pggc_cluster_data; /* interface/cluster_data.hpp:9-181   */
+
+typedef struct pggc_stats {
+    int64_t levels;      /* ExperimentLoggerUtil level count (src/clustering_methods.cpp:123)  */
+    int64_t total_nnz;   /* ExperimentLoggerUtil total nnz   (src/clustering_methods.cpp:122)  */
+    int64_t sweeps;      /* local-move sweeps executed                                        */
+    int64_t moves;       /* vertex moves applied                                              */
+    int64_t passes;      /* leiden_part / louvain_part calls (1 + ex_iters passes)            */
+    double objective;    /* cluster_data::get_objective() after the call                      */
+    double raw_obj;      /* cluster_data::obj                                                 */
+    int64_t label_count; /* cluster_data::label_count                                         */
+} pggc_stats;
+
+const char* pggc_last_error(void);
+/* build-time identification, e.g. "pggc-b200 sm_100a" */
+const char* pggc_version(void);
+
+/* ---- memory_store (interface/memory_store.hpp:84-90) ---------------------- */
+pggc_status pggc_context_create(int device, pggc_context** out);
+pggc_status pggc_context_destroy(pggc_context* ctx);
+/* the cudaStream_t all calls on this context are issued on */
+pggc_status pggc_context_stream(pggc_context* ctx, void** stream_out);
+
+/* ---- weighted_graph (interface/weighted_graph.h:10-19) --------------------
+ * Copies the CSR.  vtx_w may be NULL: the objective's default vertex weights
+ * are computed (degree for Mod, weighted degree for WMod, 1 otherwise;
+ * app/io/vertex_weighting.cpp:27-42). */
+pggc_status pggc_graph_create(pggc_context* ctx, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col,
+                              const void* weights, int weight_kind, const void* vtx_w, int objective, int mem_kind,
+                              pggc_graph** out);
+pggc_status pggc_graph_destroy(pggc_graph* g);
+pggc_status pggc_graph_dims(const pggc_graph* g, int64_t* n, int64_t* nnz, int* weight_kind);
+/* copies out any non-NULL array (weights only for non-uniform graphs) */
+pggc_status pggc_graph_read(pggc_context* ctx, const pggc_graph* g, int64_t* rowptr, int32_t* col, void* weights,
+                            void* vtx_w, int mem_kind);
+
+/* ---- cluster_data and subclasses (interface/cluster_data.hpp:38-181,
+ *      app/objective_helpers.hpp:9-22) --------------------------------------- */
+pggc_status pggc_cluster_data_create(pggc_context* ctx, const pggc_graph* g, int objective, double lambda_mult,
+                                     pggc_cluster_data** out);
+pggc_status pggc_cluster_data_destroy(pggc_cluster_data* cd);
+/* any output pointer may be NULL */
+pggc_status pggc_cluster_data_get(const pggc_cluster_data* cd, double* obj, double* objective, double* lambda,
+                                  double* uncut, int64_t* label_count);
+/* total_deg[0..label_count) */
+pggc_status pggc_cluster_data_total_deg(pggc_context* ctx, const pggc_cluster_data* cd, void* out, int mem_kind);
+/* overwrite label_count / total_deg / uncut and recompute obj */
+pggc_status pggc_cluster_data_set(pggc_context* ctx, pggc_cluster_data* cd, int64_t label_count, const void* total_deg,
+                                  double uncut, int mem_kind);
+
+/* ---- ordering::generate_orderings (src/header/ordering.h:21) -------------
+ * offsets = {offset_large, offset_large2, offset_mid, offset_mid2} */
+pggc_status pggc_generate_orderings(pggc_context* ctx, const pggc_graph* g, int32_t* order1, int32_t* order2,
+                                    int64_t offsets[4], int mem_kind);
+
+/* ---- local_move_heuristic (src/header/local_mover.h:21-25) ----------------
+ * local_move<constrained> (strict = 0) or local_move_strict<constrained>
+ * (strict = 1) on partition part_io with cluster_data cd (in/out).
+ * constraint_io (cluster-indexed, constraint_len entries with
+ * n <= constraint_len <= 2n + 64) is used when constrained; entries for labels
+ * appended by the call are written back when they fit.
+ * sweep_limit < 0: the reference schedule; >= 0 caps the sweeps (test hook). */
+pggc_status pggc_local_move(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int32_t* part_io,
+                            int is_initial, int constrained, int32_t* constraint_io, int64_t constraint_len,
+                            int enable_sa, int strict, int sweep_limit, int mem_kind, pggc_stats* stats);
+
+/* One candidates_and_destinations pass (src/local_mover.cpp:567-634) on a given
+ * state: dest_io is the dest cache in, destinations out (NO_MOVE = -3,
+ * NEW_PART = -4); gain_out receives save_gains.  pvals: own-cluster weights
+ * (V type).  initial != 0 uses the input graph as the conn graph. */
+pggc_status pggc_select_pass(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, const int32_t* part,
+                             const void* pvals, int32_t* dest_io, float* gain_out, float filter_ratio, int initial,
+                             int constrained, const int32_t* constraint, int mem_kind, int64_t* num_candidates);
+
+/* ---- contracter::build_coarse_graph (src/header/contract.h:20-24) --------
+ * Coarse CSR with rows sorted by column, self-loops dropped, weights summed;
+ * coarse vertex weights are summed vertex weights.  The new graph has int32
+ * weights (integer inputs) or float32 weights (float32 input). */
+pggc_status pggc_build_coarse_graph(pggc_context* ctx, const pggc_graph* g, const int32_t* vcmap, int64_t nc,
+                                    int mem_kind, pggc_graph** out);
+
+/* ---- leidenR::coarsen_leidenR (src/header/leidenR.h:26-31) ---------------
+ * Refines `constraint` (the local-move partition, cd its cluster_data);
+ * seed_pick / seed_order replace the two std::random_device draws. */
+pggc_status pggc_coarsen_leidenR(pggc_context* ctx, const pggc_graph* g, const pggc_cluster_data* cd,
+                                 const int32_t* constraint, uint32_t seed_pick, uint32_t seed_order,
+                                 int32_t* vcmap_out, int64_t* nc_out, int mem_kind);
+
+/* ---- clustering_methods (interface/clustering_methods.h:20-24) ----------- */
+pggc_status pggc_leiden_part(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int plus, int improve,
+                             const int32_t* input, uint64_t seed, int32_t* labels_out, int mem_kind,
+                             pggc_stats* stats);
+pggc_status pggc_louvain_part(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int constrained,
+                              const int32_t* constraint, int32_t* labels_out, int mem_kind, pggc_stats* stats);
+
+/* run_clustering (app/cluster_main.cpp:116-165): the method, then ex_iters
+ * improvement passes (ex_iters < 0: until the objective stops rising). */
+pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int method,
+                                int ex_iters, uint64_t seed, int32_t* labels_out, int mem_kind, pggc_stats* stats);
+
+/* verify_objective<uniform> (app/verify_objective.cpp:64-89) in int64 / FP64 */
+pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, int objective,
+                                  double lambda_mult, int mem_kind, double* objective_out, double* raw_obj_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PGGC_H */

@@ -72,7 +72,7 @@ def build_cuda(force: bool = False, verbose_ptxas: bool = False) -> str:
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             cmd = [_nvcc(), *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "-ccbin", _host_cxx(),
-                   "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC,
+                   "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "--extended-lambda", "-fmad=false", "-I", INCLUDE, "-I", CSRC,
                    "-c", s, "-o", o]
             if verbose_ptxas:
                 cmd[1:1] = ["-Xptxas", "-v"]

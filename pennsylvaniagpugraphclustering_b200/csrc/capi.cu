@@ -1,0 +1,677 @@
+// capi.cu -- the extern "C" boundary declared in include/pggc.h.
+#include <cstring>
+#include <string>
+#include "kernels.cuh"
+#include "pggc.h"
+
+using namespace pggc;
+
+struct pggc_context {
+    std::unique_ptr<Context> ctx;
+};
+
+struct pggc_graph {
+    pggc_context* owner = nullptr;
+    int kind = PGGC_W_UNIFORM;
+    std::unique_ptr<Graph<i32>> gi;
+    std::unique_ptr<Graph<float>> gf;
+    bool is_float() const { return kind == PGGC_W_FLOAT32; }
+};
+
+struct pggc_cluster_data {
+    bool is_float = false;
+    ClusterState<i64> ci;
+    ClusterState<double> cf;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+pggc_status fail(pggc_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+template <class F>
+pggc_status guarded(F f) {
+    try {
+        f();
+        return PGGC_OK;
+    } catch (const InvalidArg& e) {
+        return fail(PGGC_ERR_INVALID, e.what());
+    } catch (const DeviceFault& e) {
+        return fail(PGGC_ERR_DEVICE, e.what());
+    } catch (const CudaError& e) {
+        return fail(PGGC_ERR_CUDA, e.what());
+    } catch (const std::exception& e) {
+        return fail(PGGC_ERR_INTERNAL, e.what());
+    }
+}
+
+void need(bool cond, const char* what) {
+    if (!cond) throw InvalidArg(what);
+}
+
+// caller array -> device pointer (copied in for host memory)
+template <class T>
+struct In {
+    DBuf<T> tmp;
+    const T* p = nullptr;
+    In(Context& ctx, const T* src, i64 count, int mem_kind) {
+        if (!src || count <= 0) {
+            p = src;
+            return;
+        }
+        if (mem_kind == PGGC_MEM_DEVICE) {
+            p = src;
+        } else {
+            tmp = DBuf<T>(ctx, count);
+            PGGC_CUDA(cudaMemcpyAsync(tmp.p, src, sizeof(T) * (size_t)count, cudaMemcpyHostToDevice, ctx.stream));
+            p = tmp.p;
+        }
+    }
+};
+
+// caller output array: device pointer for the kernels, copied out by finish()
+template <class T>
+struct Out {
+    Context& ctx;
+    DBuf<T> tmp;
+    T* user;
+    T* p;
+    i64 count;
+    int mem_kind;
+    Out(Context& c, T* dst, i64 n, int mk, bool copy_in) : ctx(c), user(dst), p(dst), count(n), mem_kind(mk) {
+        if (mem_kind != PGGC_MEM_DEVICE && dst && n > 0) {
+            tmp = DBuf<T>(ctx, n);
+            p = tmp.p;
+            if (copy_in)
+                PGGC_CUDA(cudaMemcpyAsync(tmp.p, dst, sizeof(T) * (size_t)n, cudaMemcpyHostToDevice, ctx.stream));
+        }
+    }
+    void finish() {
+        if (mem_kind != PGGC_MEM_DEVICE && user && count > 0)
+            PGGC_CUDA(cudaMemcpyAsync(user, p, sizeof(T) * (size_t)count, cudaMemcpyDeviceToHost, ctx.stream));
+    }
+};
+
+__global__ void k_labels_in_range(const i32* labels, i64 n, i64 hi, int* bad) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        if (labels[i] < 0 || labels[i] >= hi) atomicExch(bad, 1);
+}
+
+// rejects label arrays with entries outside [0, hi) before any kernel indexes by them
+void check_labels(Context& c, const i32* labels, i64 n, i64 hi, const char* what) {
+    if (n <= 0) return;
+    DBuf<int> bad(c, 1);
+    PGGC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), c.stream));
+    k_labels_in_range<<<(int)std::min<i64>(ceil_div(n, 256), 4096), 256, 0, c.stream>>>(labels, n, hi, bad.p);
+    PGGC_LAUNCH_CHECK();
+    need(c.read1(bad.p) == 0, what);
+}
+
+void check_mem_kind(int mk) { need(mk == PGGC_MEM_HOST || mk == PGGC_MEM_DEVICE, "mem_kind must be PGGC_MEM_HOST or PGGC_MEM_DEVICE"); }
+
+template <class W>
+std::unique_ptr<Graph<W>> make_graph(Context& ctx, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col,
+                                     const void* weights, int kind, const void* vtx_w, int objective, int mem_kind) {
+    using V = typename Traits<W>::V;
+    auto g = std::make_unique<Graph<W>>();
+    g->n = n;
+    g->nnz = nnz;
+    g->uniform = kind == PGGC_W_UNIFORM;
+    g->rowptr = DBuf<i64>(ctx, n + 1);
+    g->col = DBuf<i32>(ctx, std::max<i64>(nnz, 1));
+    auto kindc = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    PGGC_CUDA(cudaMemcpyAsync(g->rowptr.p, rowptr, sizeof(i64) * (n + 1), kindc, ctx.stream));
+    if (nnz > 0) PGGC_CUDA(cudaMemcpyAsync(g->col.p, col, sizeof(i32) * nnz, kindc, ctx.stream));
+    if (!g->uniform) {
+        need(weights != nullptr, "weights required for a non-uniform graph");
+        g->w = DBuf<W>(ctx, std::max<i64>(nnz, 1));
+        if (nnz > 0) PGGC_CUDA(cudaMemcpyAsync(g->w.p, weights, sizeof(W) * nnz, kindc, ctx.stream));
+    }
+    if (vtx_w) {
+        g->vtx_w = DBuf<V>(ctx, std::max<i64>(n, 1));
+        if (n > 0) PGGC_CUDA(cudaMemcpyAsync(g->vtx_w.p, vtx_w, sizeof(V) * n, kindc, ctx.stream));
+    } else {
+        default_vertex_weights<W>(ctx, *g, objective);
+    }
+    ctx.sync();
+    return g;
+}
+
+void validate_csr_host(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col) {
+    need(rowptr[0] == 0, "rowptr[0] must be 0");
+    need(rowptr[n] == nnz, "rowptr[n] must equal nnz");
+    for (int64_t i = 0; i < n; i++) {
+        need(rowptr[i + 1] >= rowptr[i], "rowptr must be non-decreasing");
+        for (int64_t j = rowptr[i]; j < rowptr[i + 1]; j++) {
+            need(col[j] >= 0 && col[j] < n, "column index out of range");
+            need(col[j] != i, "self-loops are not supported");
+        }
+    }
+}
+
+template <class F>
+void dispatch(const pggc_graph* g, F f) {
+    if (g->is_float()) f(*g->gf, (double*)nullptr);
+    else f(*g->gi, (i64*)nullptr);
+}
+
+template <class V>
+ClusterState<V>& cstate(pggc_cluster_data* cd);
+template <>
+ClusterState<i64>& cstate<i64>(pggc_cluster_data* cd) {
+    return cd->ci;
+}
+template <>
+ClusterState<double>& cstate<double>(pggc_cluster_data* cd) {
+    return cd->cf;
+}
+
+void fill_stats(pggc_stats* st, const RunStats& rs, double objective, double raw, i64 L) {
+    if (!st) return;
+    st->levels = rs.levels;
+    st->total_nnz = rs.total_nnz;
+    st->sweeps = rs.sweeps;
+    st->moves = rs.moves;
+    st->passes = rs.passes;
+    st->objective = objective;
+    st->raw_obj = raw;
+    st->label_count = L;
+}
+
+// verify_objective kernels
+template <class W>
+__global__ void k_verify_totals(DGraph<W> g, const i32* labels, typename Traits<W>::V* total) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < g.n; i += (i64)gridDim.x * blockDim.x) {
+        if constexpr (std::is_same<typename Traits<W>::V, double>::value) ::atomicAdd(&total[labels[i]], g.vtx_w[i]);
+        else ::atomicAdd((unsigned long long*)&total[labels[i]], (unsigned long long)g.vtx_w[i]);
+    }
+}
+__global__ void k_check_labels(const i32* labels, i64 n, int* bad) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        if (labels[i] < 0 || labels[i] >= n) atomicExch(bad, 1);
+}
+struct I64Arr {
+    const i64* a;
+    __device__ i64 operator()(i64 i) const { return a[i]; }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* pggc_last_error(void) { return g_last_error.c_str(); }
+const char* pggc_version(void) { return "pggc-b200 0.1 sm_100a"; }
+
+pggc_status pggc_context_create(int device, pggc_context** out) {
+    return guarded([&] {
+        need(out != nullptr, "out is NULL");
+        int count = 0;
+        PGGC_CUDA(cudaGetDeviceCount(&count));
+        need(device >= 0 && device < count, "device index out of range");
+        auto* c = new pggc_context();
+        try {
+            c->ctx = std::make_unique<Context>(device);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+pggc_status pggc_context_destroy(pggc_context* ctx) {
+    return guarded([&] { delete ctx; });
+}
+
+pggc_status pggc_context_stream(pggc_context* ctx, void** stream_out) {
+    return guarded([&] {
+        need(ctx && stream_out, "NULL argument");
+        *stream_out = (void*)ctx->ctx->stream;
+    });
+}
+
+pggc_status pggc_graph_create(pggc_context* ctx, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col,
+                              const void* weights, int weight_kind, const void* vtx_w, int objective, int mem_kind,
+                              pggc_graph** out) {
+    return guarded([&] {
+        need(ctx && out && rowptr, "NULL argument");
+        need(n >= 0 && n < 2147483647 && nnz >= 0, "n must be in [0, 2^31-1) and nnz >= 0");
+        need(nnz == 0 || col != nullptr, "col is NULL");
+        need(weight_kind >= PGGC_W_UNIFORM && weight_kind <= PGGC_W_FLOAT32, "unknown weight kind");
+        need(objective >= PGGC_OBJ_MOD && objective <= PGGC_OBJ_LCC, "unknown objective");
+        check_mem_kind(mem_kind);
+        if (mem_kind == PGGC_MEM_HOST) validate_csr_host(n, nnz, rowptr, col);
+        Context& c = *ctx->ctx;
+        c.sync();
+        auto* g = new pggc_graph();
+        g->owner = ctx;
+        g->kind = weight_kind;
+        try {
+            if (weight_kind == PGGC_W_FLOAT32)
+                g->gf = make_graph<float>(c, n, nnz, rowptr, col, weights, weight_kind, vtx_w, objective, mem_kind);
+            else
+                g->gi = make_graph<i32>(c, n, nnz, rowptr, col, weights, weight_kind, vtx_w, objective, mem_kind);
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        *out = g;
+    });
+}
+
+pggc_status pggc_graph_destroy(pggc_graph* g) {
+    return guarded([&] { delete g; });
+}
+
+pggc_status pggc_graph_dims(const pggc_graph* g, int64_t* n, int64_t* nnz, int* weight_kind) {
+    return guarded([&] {
+        need(g != nullptr, "NULL graph");
+        i64 nn = g->is_float() ? g->gf->n : g->gi->n;
+        i64 mm = g->is_float() ? g->gf->nnz : g->gi->nnz;
+        if (n) *n = nn;
+        if (nnz) *nnz = mm;
+        if (weight_kind) *weight_kind = g->kind;
+    });
+}
+
+pggc_status pggc_graph_read(pggc_context* ctx, const pggc_graph* g, int64_t* rowptr, int32_t* col, void* weights,
+                            void* vtx_w, int mem_kind) {
+    return guarded([&] {
+        need(ctx && g, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        auto kindc = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
+            auto gv = gr.view();
+            if (rowptr) PGGC_CUDA(cudaMemcpyAsync(rowptr, gv.rowptr, sizeof(i64) * (gr.n + 1), kindc, c.stream));
+            if (col && gr.nnz) PGGC_CUDA(cudaMemcpyAsync(col, gv.col, sizeof(i32) * gr.nnz, kindc, c.stream));
+            if (weights && gv.w && gr.nnz) PGGC_CUDA(cudaMemcpyAsync(weights, gv.w, sizeof(W) * gr.nnz, kindc, c.stream));
+            if (vtx_w && gr.n) PGGC_CUDA(cudaMemcpyAsync(vtx_w, gv.vtx_w, sizeof(V) * gr.n, kindc, c.stream));
+        });
+        c.sync();
+    });
+}
+
+pggc_status pggc_cluster_data_create(pggc_context* ctx, const pggc_graph* g, int objective, double lambda_mult,
+                                     pggc_cluster_data** out) {
+    return guarded([&] {
+        need(ctx && g && out, "NULL argument");
+        need(objective >= PGGC_OBJ_MOD && objective <= PGGC_OBJ_LCC, "unknown objective");
+        Context& c = *ctx->ctx;
+        auto* cd = new pggc_cluster_data();
+        try {
+            cd->is_float = g->is_float();
+            if (g->is_float()) make_cluster_state<float>(c, *g->gf, objective, lambda_mult, cd->cf);
+            else make_cluster_state<i32>(c, *g->gi, objective, lambda_mult, cd->ci);
+            c.sync();
+        } catch (...) {
+            delete cd;
+            throw;
+        }
+        *out = cd;
+    });
+}
+
+pggc_status pggc_cluster_data_destroy(pggc_cluster_data* cd) {
+    return guarded([&] { delete cd; });
+}
+
+pggc_status pggc_cluster_data_get(const pggc_cluster_data* cd, double* obj, double* objective, double* lambda,
+                                  double* uncut, int64_t* label_count) {
+    return guarded([&] {
+        need(cd != nullptr, "NULL cluster_data");
+        auto get = [&](const auto& cs) {
+            if (obj) *obj = cs.obj;
+            if (objective) *objective = cs.get_objective();
+            if (lambda) *lambda = cs.lambda;
+            if (uncut) *uncut = (double)cs.uncut;
+            if (label_count) *label_count = cs.label_count;
+        };
+        if (cd->is_float) get(cd->cf);
+        else get(cd->ci);
+    });
+}
+
+pggc_status pggc_cluster_data_total_deg(pggc_context* ctx, const pggc_cluster_data* cd, void* out, int mem_kind) {
+    return guarded([&] {
+        need(ctx && cd && out, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        auto kindc = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (cd->is_float)
+            PGGC_CUDA(cudaMemcpyAsync(out, cd->cf.total_deg.p, sizeof(double) * cd->cf.label_count, kindc, c.stream));
+        else
+            PGGC_CUDA(cudaMemcpyAsync(out, cd->ci.total_deg.p, sizeof(i64) * cd->ci.label_count, kindc, c.stream));
+        c.sync();
+    });
+}
+
+pggc_status pggc_cluster_data_set(pggc_context* ctx, pggc_cluster_data* cd, int64_t label_count, const void* total_deg,
+                                  double uncut, int mem_kind) {
+    return guarded([&] {
+        need(ctx && cd && total_deg, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        auto kindc = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        auto set = [&](auto& cs, size_t elem) {
+            need(label_count >= 0 && label_count <= cs.capacity, "label_count exceeds capacity");
+            PGGC_CUDA(cudaMemcpyAsync(cs.total_deg.p, total_deg, elem * label_count, kindc, c.stream));
+            cs.label_count = label_count;
+            using V = std::remove_reference_t<decltype(cs.uncut)>;
+            cs.uncut = (V)uncut;
+            update_objective(c, cs);
+        };
+        if (cd->is_float) set(cd->cf, sizeof(double));
+        else set(cd->ci, sizeof(i64));
+        c.sync();
+    });
+}
+
+pggc_status pggc_generate_orderings(pggc_context* ctx, const pggc_graph* g, int32_t* order1, int32_t* order2,
+                                    int64_t offsets[4], int mem_kind) {
+    return guarded([&] {
+        need(ctx && g, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        Ordering o;
+        dispatch(g, [&](auto& gr, auto*) { generate_orderings(c, gr.view().rowptr, gr.n, o); });
+        auto kindc = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (o.n > 0) {
+            if (order1) PGGC_CUDA(cudaMemcpyAsync(order1, o.order1.p, sizeof(i32) * o.n, kindc, c.stream));
+            if (order2) PGGC_CUDA(cudaMemcpyAsync(order2, o.order2.p, sizeof(i32) * o.n, kindc, c.stream));
+        }
+        if (offsets) {
+            offsets[0] = o.off_large;
+            offsets[1] = o.off_large2;
+            offsets[2] = o.off_mid;
+            offsets[3] = o.off_mid2;
+        }
+        c.sync();
+    });
+}
+
+pggc_status pggc_local_move(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int32_t* part_io,
+                            int is_initial, int constrained, int32_t* constraint_io, int64_t constraint_len,
+                            int enable_sa, int strict, int sweep_limit, int mem_kind, pggc_stats* stats) {
+    return guarded([&] {
+        need(ctx && g && cd && part_io, "NULL argument");
+        need(!constrained || constraint_io, "constraint required when constrained");
+        need(cd->is_float == g->is_float(), "cluster_data / graph weight kinds differ");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            auto& cs = cstate<V>(cd);
+            need(!constrained || (constraint_len >= cs.label_count && constraint_len <= cs.capacity),
+                 "constraint_len must lie in [label_count, 2n + 64]");
+            need(!constrained || constraint_len >= gr.n, "constraint_len must be >= n");
+            Out<i32> part(c, part_io, gr.n, mem_kind, true);
+            check_labels(c, part.p, gr.n, cs.label_count, "partition labels must lie in [0, label_count)");
+            // cluster-indexed constraint with room for appended labels
+            DBuf<i32> con;
+            if (constrained) {
+                con = DBuf<i32>(c, cs.capacity);
+                PGGC_CUDA(cudaMemsetAsync(con.p, 0, sizeof(i32) * cs.capacity, c.stream));
+                auto k = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+                PGGC_CUDA(cudaMemcpyAsync(con.p, constraint_io, sizeof(i32) * constraint_len, k, c.stream));
+            }
+            Ordering o;
+            generate_orderings(c, gr.view().rowptr, gr.n, o);
+            MoveStats ms;
+            local_move(c, gr, o, part.p, cs, is_initial != 0, constrained != 0, constrained ? con.p : nullptr,
+                       enable_sa != 0, strict != 0, sweep_limit, &ms);
+            part.finish();
+            if (constrained) {
+                auto k = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+                PGGC_CUDA(cudaMemcpyAsync(constraint_io, con.p, sizeof(i32) * constraint_len, k, c.stream));
+            }
+            c.sync();
+            RunStats rs;
+            rs.sweeps = ms.sweeps;
+            rs.moves = ms.moves;
+            fill_stats(stats, rs, cs.get_objective(), cs.obj, cs.label_count);
+        });
+    });
+}
+
+pggc_status pggc_select_pass(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, const int32_t* part,
+                             const void* pvals, int32_t* dest_io, float* gain_out, float filter_ratio, int initial,
+                             int constrained, const int32_t* constraint, int mem_kind, int64_t* num_candidates) {
+    return guarded([&] {
+        need(ctx && g && cd && part && pvals && dest_io && gain_out, "NULL argument");
+        need(cd->is_float == g->is_float(), "cluster_data / graph weight kinds differ");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            auto& cs = cstate<V>(cd);
+            In<i32> pin(c, part, gr.n, mem_kind);
+            In<V> pv(c, (const V*)pvals, gr.n, mem_kind);
+            DBuf<i32> con;
+            if (constrained) {
+                con = DBuf<i32>(c, cs.capacity);
+                PGGC_CUDA(cudaMemsetAsync(con.p, 0, sizeof(i32) * cs.capacity, c.stream));
+                auto k = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+                PGGC_CUDA(cudaMemcpyAsync(con.p, constraint, sizeof(i32) * cs.label_count, k, c.stream));
+            }
+            check_labels(c, pin.p, gr.n, cs.label_count, "partition labels must lie in [0, label_count)");
+            Out<i32> dest(c, dest_io, gr.n, mem_kind, true);
+            Out<float> gain(c, gain_out, gr.n, mem_kind, false);
+            Ordering o;
+            generate_orderings(c, gr.view().rowptr, gr.n, o);
+            i64 k = select_pass(c, gr, o, pin.p, pv.p, cs, dest.p, gain.p, filter_ratio, initial != 0,
+                                constrained != 0, con.p);
+            dest.finish();
+            gain.finish();
+            c.sync();
+            if (num_candidates) *num_candidates = k;
+        });
+    });
+}
+
+pggc_status pggc_build_coarse_graph(pggc_context* ctx, const pggc_graph* g, const int32_t* vcmap, int64_t nc,
+                                    int mem_kind, pggc_graph** out) {
+    return guarded([&] {
+        need(ctx && g && vcmap && out, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        auto* cg = new pggc_graph();
+        cg->owner = ctx;
+        try {
+            dispatch(g, [&](auto& gr, auto* vtag) {
+                using V = std::remove_pointer_t<decltype(vtag)>;
+                need(nc >= 0 && nc <= gr.n, "nc out of range");
+                In<i32> map(c, vcmap, gr.n, mem_kind);
+                check_labels(c, map.p, gr.n, nc, "vcmap entries must lie in [0, nc)");
+                auto next = build_coarse_graph(c, gr, map.p, nc);
+                coarsen_vtx_w(c, gr, map.p, *next);
+                c.sync();
+                if constexpr (std::is_same<V, double>::value) {
+                    cg->kind = PGGC_W_FLOAT32;
+                    cg->gf = std::move(next);
+                } else {
+                    cg->kind = PGGC_W_INT32;
+                    cg->gi = std::move(next);
+                }
+            });
+        } catch (...) {
+            delete cg;
+            throw;
+        }
+        *out = cg;
+    });
+}
+
+pggc_status pggc_coarsen_leidenR(pggc_context* ctx, const pggc_graph* g, const pggc_cluster_data* cd,
+                                 const int32_t* constraint, uint32_t seed_pick, uint32_t seed_order,
+                                 int32_t* vcmap_out, int64_t* nc_out, int mem_kind) {
+    return guarded([&] {
+        need(ctx && g && cd && constraint && vcmap_out, "NULL argument");
+        need(cd->is_float == g->is_float(), "cluster_data / graph weight kinds differ");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            auto& cs = cstate<V>(const_cast<pggc_cluster_data*>(cd));
+            In<i32> con(c, constraint, gr.n, mem_kind);
+            check_labels(c, con.p, gr.n, cs.label_count, "constraint labels must lie in [0, label_count)");
+            Out<i32> vc(c, vcmap_out, gr.n, mem_kind, false);
+            Ordering o;
+            generate_orderings(c, gr.view().rowptr, gr.n, o);
+            i64 nc = coarsen_leidenR(c, gr, o, con.p, cs, seed_pick, seed_order, vc.p);
+            vc.finish();
+            c.sync();
+            if (nc_out) *nc_out = nc;
+        });
+    });
+}
+
+pggc_status pggc_leiden_part(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int plus, int improve,
+                             const int32_t* input, uint64_t seed, int32_t* labels_out, int mem_kind,
+                             pggc_stats* stats) {
+    return guarded([&] {
+        need(ctx && g && cd && labels_out, "NULL argument");
+        need(!improve || input, "input partition required when improve");
+        need(cd->is_float == g->is_float(), "cluster_data / graph weight kinds differ");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            auto& cs = cstate<V>(cd);
+            In<i32> inp(c, improve ? input : nullptr, gr.n, mem_kind);
+            if (improve) check_labels(c, inp.p, gr.n, cs.label_count, "input labels must lie in [0, label_count)");
+            Out<i32> lab(c, labels_out, gr.n, mem_kind, false);
+            RunStats rs;
+            rs.passes = 1;
+            leiden_part(c, gr, cs, plus != 0, improve != 0, inp.p, seed, lab.p, &rs);
+            lab.finish();
+            c.sync();
+            fill_stats(stats, rs, cs.get_objective(), cs.obj, cs.label_count);
+        });
+    });
+}
+
+pggc_status pggc_louvain_part(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int constrained,
+                              const int32_t* constraint, int32_t* labels_out, int mem_kind, pggc_stats* stats) {
+    return guarded([&] {
+        need(ctx && g && cd && labels_out, "NULL argument");
+        need(!constrained || constraint, "constraint required when constrained");
+        need(cd->is_float == g->is_float(), "cluster_data / graph weight kinds differ");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            auto& cs = cstate<V>(cd);
+            In<i32> con(c, constrained ? constraint : nullptr, gr.n, mem_kind);
+            if (constrained) check_labels(c, con.p, gr.n, gr.n, "constraint labels must lie in [0, n)");
+            Out<i32> lab(c, labels_out, gr.n, mem_kind, false);
+            RunStats rs;
+            rs.passes = 1;
+            louvain_part(c, gr, cs, constrained != 0, con.p, lab.p, &rs);
+            lab.finish();
+            c.sync();
+            fill_stats(stats, rs, cs.get_objective(), cs.obj, cs.label_count);
+        });
+    });
+}
+
+pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int method,
+                                int ex_iters, uint64_t seed, int32_t* labels_out, int mem_kind, pggc_stats* stats) {
+    return guarded([&] {
+        need(ctx && g && cd && labels_out, "NULL argument");
+        need(method >= PGGC_METHOD_LOUVAIN && method <= PGGC_METHOD_LEIDEN_PLUS, "unknown method");
+        need(cd->is_float == g->is_float(), "cluster_data / graph weight kinds differ");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            auto& cs = cstate<V>(cd);
+            const i64 n = gr.n;
+            Out<i32> lab(c, labels_out, n, mem_kind, false);
+            DBuf<i32> part(c, std::max<i64>(n, 1)), con(c, std::max<i64>(n, 1));
+            RunStats rs;
+            u64 pass = 0;
+            auto one = [&](bool improve) {
+                RunStats r1;
+                if (method == PGGC_METHOD_LOUVAIN) {
+                    louvain_part(c, gr, cs, improve, con.p, part.p, &r1);
+                } else {
+                    u64 s = seed + 0x9E3779B97F4A7C15ull * pass;
+                    pass++;
+                    leiden_part(c, gr, cs, method == PGGC_METHOD_LEIDEN_PLUS, improve, con.p, s, part.p, &r1);
+                }
+                rs.levels = r1.levels;
+                rs.total_nnz = r1.total_nnz;
+                rs.sweeps += r1.sweeps;
+                rs.moves += r1.moves;
+                rs.passes++;
+            };
+            one(false);
+            double last = -std::numeric_limits<double>::infinity();
+            int counter = 0;
+            while (true) {
+                bool terminate = true;
+                if (ex_iters < 0) {
+                    if (cs.get_objective() > last) terminate = false;
+                    last = cs.get_objective();
+                } else {
+                    if (counter++ < ex_iters) terminate = false;
+                }
+                if (terminate) break;
+                copy_d2d(c, con.p, part.p, n);
+                one(true);
+            }
+            copy_d2d(c, lab.p, part.p, n);
+            lab.finish();
+            c.sync();
+            fill_stats(stats, rs, cs.get_objective(), cs.obj, cs.label_count);
+        });
+    });
+}
+
+pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, int objective,
+                                  double lambda_mult, int mem_kind, double* objective_out, double* raw_obj_out) {
+    return guarded([&] {
+        need(ctx && g && labels, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
+            const i64 n = gr.n;
+            In<i32> lab(c, labels, n, mem_kind);
+            DBuf<int> bad(c, 1);
+            PGGC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), c.stream));
+            if (n > 0) k_check_labels<<<(int)std::min<i64>(ceil_div(n, 256), 4096), 256, 0, c.stream>>>(lab.p, n, bad.p);
+            need(c.read1(bad.p) == 0, "labels must lie in [0, n)");
+            ClusterState<V> cs;
+            make_cluster_state<W>(c, gr, objective, lambda_mult, cs);
+            PGGC_CUDA(cudaMemsetAsync(cs.total_deg.p, 0, sizeof(V) * cs.capacity, c.stream));
+            if (n > 0) {
+                k_verify_totals<W><<<(int)std::min<i64>(ceil_div(n, 256), 4096), 256, 0, c.stream>>>(gr.view(), lab.p,
+                                                                                                     cs.total_deg.p);
+                PGGC_LAUNCH_CHECK();
+            }
+            Ordering o;
+            generate_orderings(c, gr.view().rowptr, n, o);
+            DBuf<V> own(c, std::max<i64>(n, 1));
+            own_weights<W>(c, gr, o, lab.p, own.p);
+            DBuf<V> u(c, 1);
+            if constexpr (std::is_same<V, double>::value) det_reduce(c, DArrIn{own.p}, n, u.p);
+            else sum_i64(c, I64Arr{own.p}, n, u.p);
+            cs.uncut = c.read1(u.p);
+            cs.label_count = n;
+            update_objective(c, cs);
+            if (objective_out) *objective_out = cs.get_objective();
+            if (raw_obj_out) *raw_obj_out = cs.obj;
+        });
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,350 @@
+// driver.cu -- objective state and the multilevel V-cycles
+// (src/clustering_methods.cpp:33-222, interface/cluster_data.hpp:76-181,
+//  app/io/vertex_weighting.cpp:27-42).
+//
+// The host C++ here plays the role of clustering_methods::leiden_part /
+// louvain_part: it owns the level hierarchy (device-resident coarse graphs and
+// coarse maps) and sequences the kernel families.  Decisions the reference
+// makes on host scalars (objective unchanged, label_count == n, coarse count)
+// stay on the host; everything else stays on the device.
+#include "kernels.cuh"
+
+namespace pggc {
+
+// ---------------------------------------------------------------------------
+// objective state
+// ---------------------------------------------------------------------------
+template <class V>
+struct SqAll;
+template <>
+struct SqAll<i64> {
+    const i64* td;
+    __device__ i64 operator()(i64 i) const { return td[i] * td[i]; }
+};
+template <>
+struct SqAll<double> {
+    const double* td;
+    __device__ double operator()(i64 i) const { return td[i] * td[i]; }
+};
+struct I64In {
+    const i64* a;
+    __device__ i64 operator()(i64 i) const { return a[i]; }
+};
+struct I32WIn {
+    const i32* a;
+    __device__ i64 operator()(i64 i) const { return a[i]; }
+};
+struct FWIn {
+    const float* a;
+    __device__ double operator()(i64 i) const { return (double)a[i]; }
+};
+
+template <class V>
+void update_objective(Context& ctx, ClusterState<V>& cs) {
+    DBuf<i64> si(ctx, 1);
+    DBuf<double> sd(ctx, 1);
+    double m;
+    if constexpr (std::is_same<V, i64>::value) {
+        sum_i64(ctx, SqAll<i64>{cs.total_deg.p}, cs.label_count, si.p);
+        i64 ss = ctx.read1(si.p);
+        m = static_cast<double>(cs.uncut);
+        m = m - cs.lambda * static_cast<double>(ss);
+    } else {
+        det_reduce(ctx, SqAll<double>{cs.total_deg.p}, cs.label_count, sd.p);
+        double ss = ctx.read1(sd.p);
+        m = cs.uncut;
+        m = m - cs.lambda * ss;
+    }
+    cs.obj = m;
+}
+
+template <class W>
+__global__ void k_vw_warp(DGraph<W> g, int objective, typename Traits<W>::V* out) {
+    using V = typename Traits<W>::V;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 i = gw; i < g.n; i += nw) {
+        i64 b = g.rowptr[i], e = g.rowptr[i + 1];
+        V r;
+        if (objective == OBJ_MOD) r = V(e - b);
+        else if (objective == OBJ_WMOD) {
+            if constexpr (std::is_same<V, double>::value) {
+                if (e - b < MASSIVE_CUTOFF) r = (double)(float)warp_canon_sum(b, e, [&](i64 j) { return (double)g.wgt(j); });
+                else r = -1.0;  // massive rows: k_vw_block
+            } else {
+                r = warp_int_sum(b, e, [&](i64 j) -> i64 { return g.wgt(j); });
+            }
+        } else r = V(1);
+        if (lane_id() == 0 && !(std::is_same<V, double>::value && objective == OBJ_WMOD && e - b >= MASSIVE_CUTOFF))
+            out[i] = r;
+    }
+}
+template <class W>
+__global__ void __launch_bounds__(1024) k_vw_block(DGraph<W> g, const i32* list, i64 count, double* out) {
+    __shared__ double red[32];
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        i32 i = list[x];
+        double r = block1024_canon_sum(g.rowptr[i], g.rowptr[i + 1], [&](i64 j) { return (double)g.wgt(j); }, red);
+        if (threadIdx.x == 0) out[i] = (double)(float)r;
+        __syncthreads();
+    }
+}
+
+// app/io/vertex_weighting.cpp:27-42
+template <class W>
+void default_vertex_weights(Context& ctx, Graph<W>& g, int objective) {
+    using V = typename Traits<W>::V;
+    g.vtx_w = DBuf<V>(ctx, std::max<i64>(g.n, 1));
+    if (g.n == 0) return;
+    auto gv = g.view();
+    gv.vtx_w = g.vtx_w.p;
+    int grid = (int)std::min<i64>(ceil_div(ceil_div(g.n, 32), 8), (i64)ctx.num_sms * 16);
+    k_vw_warp<W><<<grid, 256, 0, ctx.stream>>>(gv, objective, g.vtx_w.p);
+    PGGC_LAUNCH_CHECK();
+    if constexpr (std::is_same<V, double>::value) {
+        if (objective == OBJ_WMOD) {
+            Ordering ord;
+            generate_orderings(ctx, gv.rowptr, g.n, ord);
+            i64 nm = g.n - ord.off_large2;
+            if (nm > 0) {
+                k_vw_block<W><<<(int)std::min<i64>(nm, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(
+                    gv, ord.order1.p + ord.off_large2, nm, g.vtx_w.p);
+                PGGC_LAUNCH_CHECK();
+            }
+        }
+    }
+}
+
+template <class W>
+void make_cluster_state(Context& ctx, const Graph<W>& g, int kind, double mult, ClusterState<typename Traits<W>::V>& cs) {
+    using V = typename Traits<W>::V;
+    cs.capacity = 2 * std::max<i64>(g.n, 1) + 64;
+    cs.total_deg = DBuf<V>(ctx, cs.capacity);
+    PGGC_CUDA(cudaMemsetAsync(cs.total_deg.p, 0, sizeof(V) * cs.capacity, ctx.stream));
+    copy_d2d(ctx, cs.total_deg.p, g.vtx_w.p, g.n);
+    cs.top_nnz = g.nnz;
+    cs.uncut = 0;
+    cs.label_count = g.n;
+    cs.kind = kind;
+    cs.lambda = 1.0;
+    DBuf<i64> si(ctx, 1);
+    DBuf<double> sd(ctx, 1);
+    auto sum_vw = [&]() -> double {
+        if constexpr (std::is_same<V, i64>::value) {
+            sum_i64(ctx, I64In{g.vtx_w.p}, g.n, si.p);
+            return (double)ctx.read1(si.p);
+        } else {
+            det_reduce(ctx, DArrIn{g.vtx_w.p}, g.n, sd.p);
+            return ctx.read1(sd.p);
+        }
+    };
+    if (kind == OBJ_MOD || kind == OBJ_WMOD) {
+        double gdeg = g.uniform ? (double)g.nnz : sum_vw();
+        cs.inv_gdeg = 1.0 / gdeg;
+        cs.lambda = mult * cs.inv_gdeg;
+    } else if (kind == OBJ_CPM) {
+        cs.v_total = (double)g.n;
+        cs.lambda = mult * 0.5;
+    } else if (kind == OBJ_NLCC) {
+        double gd;
+        if (g.uniform) gd = (double)g.nnz;
+        else {
+            if constexpr (std::is_same<V, i64>::value) {
+                sum_i64(ctx, I32WIn{(const i32*)g.view().w}, g.nnz, si.p);
+                gd = (double)ctx.read1(si.p);
+            } else {
+                det_reduce(ctx, FWIn{(const float*)g.view().w}, g.nnz, sd.p);
+                gd = ctx.read1(sd.p);
+            }
+        }
+        cs.g_deg = gd;
+        double denom;
+        if constexpr (std::is_same<V, i64>::value) {
+            sum_i64(ctx, I64In{g.vtx_w.p}, g.n, si.p);
+            u64 vt = (u64)ctx.read1(si.p);
+            denom = static_cast<double>(vt * vt);
+        } else {
+            double vt = sum_vw();
+            denom = vt * vt;
+        }
+        cs.lambda = mult * gd / denom;
+    } else {
+        cs.lambda = mult;
+    }
+    update_objective(ctx, cs);
+}
+
+// ---------------------------------------------------------------------------
+// small kernels of the V-cycle
+// ---------------------------------------------------------------------------
+__global__ void k_downsample(i64 n, const i32* in, const i32* map, i32* out) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) out[map[i]] = in[i];
+}
+__global__ void k_project(i64 n, i32* fine, const i32* coarse) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n; x += (i64)gridDim.x * blockDim.x)
+        fine[x] = coarse[fine[x]];
+}
+inline int vgrid(Context& ctx, i64 n) { return (int)std::max<i64>(1, std::min<i64>(ceil_div(n, 256), (i64)ctx.num_sms * 16)); }
+
+// leiden_part<plus,improve> (src/clustering_methods.cpp:47-137)
+template <class W>
+void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool plus, bool improve,
+                 const i32* input, u64 seed, i32* labels_out, RunStats* st) {
+    std::vector<std::unique_ptr<Graph<W>>> coarse;
+    std::vector<const Graph<W>*> levels;
+    std::vector<DBuf<i32>> parts;
+    levels.push_back(&top);
+    const i64 n = top.n;
+    DBuf<i32> part(ctx, std::max<i64>(n, 1));
+    if (!improve) iota<i32>(ctx, part.p, n);
+    else copy_d2d(ctx, part.p, input, n);
+    SplitMix64 rng(seed);
+    Ordering ord;
+    MoveStats ms;
+    while (true) {
+        const Graph<W>& c = *levels.back();
+        double old_obj = rfd.obj;
+        bool init = !improve && levels.size() == 1;
+        generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, true, false, -1, &ms);
+        if (c.nnz > 100000 && old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, false, -1, &ms);
+        if (old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, true, -1, &ms);
+        if (rfd.label_count == c.n) {
+            parts.push_back(std::move(part));
+            break;
+        }
+        u32 s_pick = (u32)rng.next();
+        u32 s_order = (u32)rng.next();
+        DBuf<i32> cmap(ctx, std::max<i64>(c.n, 1));
+        i64 nc = coarsen_leidenR<W>(ctx, c, ord, part.p, rfd, s_pick, s_order, cmap.p);
+        if (nc < c.n) {
+            auto next = build_coarse_graph<W>(ctx, c, cmap.p, nc);
+            coarsen_vtx_w<W>(ctx, c, cmap.p, *next);
+            DBuf<i32> np(ctx, std::max<i64>(nc, 1));
+            k_downsample<<<vgrid(ctx, c.n), 256, 0, ctx.stream>>>(c.n, part.p, cmap.p, np.p);
+            PGGC_LAUNCH_CHECK();
+            parts.push_back(std::move(cmap));
+            part = std::move(np);
+            levels.push_back(next.get());
+            coarse.push_back(std::move(next));
+        } else {
+            parts.push_back(std::move(cmap));
+            levels.push_back(&c);
+        }
+    }
+    if (st) {
+        st->levels = (i64)levels.size();
+        i64 t = 0;
+        for (auto* l : levels) t += l->nnz;
+        st->total_nnz = t;
+    }
+    for (i64 i = (i64)levels.size() - 2; i >= 0; i--) {
+        const Graph<W>& c = *levels[i];
+        k_project<<<vgrid(ctx, c.n), 256, 0, ctx.stream>>>(c.n, parts[i].p, parts[i + 1].p);
+        PGGC_LAUNCH_CHECK();
+        if (plus) {
+            generate_orderings(ctx, c.view().rowptr, c.n, ord);
+            local_move<W>(ctx, c, ord, parts[i].p, rfd, false, false, nullptr, true, false, -1, &ms);
+        }
+    }
+    copy_d2d(ctx, labels_out, parts[0].p, n);
+    if (st) {
+        st->sweeps += ms.sweeps;
+        st->moves += ms.moves;
+    }
+}
+
+// louvain_part<constrained> (src/clustering_methods.cpp:139-222)
+template <class W>
+void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool constrained,
+                  const i32* constraint_in, i32* labels_out, RunStats* st) {
+    using V = typename Traits<W>::V;
+    if (constrained) {
+        // cluster_data::reset (interface/cluster_data.hpp:48-54)
+        copy_d2d(ctx, rfd.total_deg.p, top.vtx_w.p, top.n);
+        rfd.uncut = 0;
+        rfd.label_count = top.n;
+        update_objective(ctx, rfd);
+    }
+    std::vector<std::unique_ptr<Graph<W>>> coarse;
+    std::vector<const Graph<W>*> levels;
+    std::vector<DBuf<i32>> parts;
+    levels.push_back(&top);
+    bool drop = constrained;
+    DBuf<i32> constraint;
+    if (constrained) {
+        constraint = DBuf<i32>(ctx, rfd.capacity);
+        PGGC_CUDA(cudaMemsetAsync(constraint.p, 0, sizeof(i32) * constraint.n, ctx.stream));
+        copy_d2d(ctx, constraint.p, constraint_in, top.n);
+    }
+    Ordering ord;
+    MoveStats ms;
+    while (true) {
+        const Graph<W>& c = *levels.back();
+        DBuf<i32> part(ctx, std::max<i64>(c.n, 1));
+        iota<i32>(ctx, part.p, c.n);
+        generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        local_move<W>(ctx, c, ord, part.p, rfd, true, constrained, constrained ? constraint.p : nullptr, true, false, -1,
+                      &ms);
+        if (constrained && rfd.label_count == c.n)
+            local_move<W>(ctx, c, ord, part.p, rfd, true, constrained, constraint.p, false, true, -1, &ms);
+        i64 L = rfd.label_count;
+        parts.push_back(std::move(part));
+        if (L < c.n) {
+            auto next = build_coarse_graph<W>(ctx, c, parts.back().p, L);
+            next->vtx_w = DBuf<V>(ctx, std::max<i64>(L, 1));
+            copy_d2d(ctx, next->vtx_w.p, rfd.total_deg.p, L);
+            levels.push_back(next.get());
+            coarse.push_back(std::move(next));
+            if (constrained) {
+                DBuf<i32> nxt(ctx, rfd.capacity);
+                PGGC_CUDA(cudaMemsetAsync(nxt.p, 0, sizeof(i32) * nxt.n, ctx.stream));
+                k_downsample<<<vgrid(ctx, c.n), 256, 0, ctx.stream>>>(c.n, constraint.p, parts.back().p, nxt.p);
+                PGGC_LAUNCH_CHECK();
+                constraint = std::move(nxt);
+            }
+        } else if (drop) {
+            PGGC_CUDA(cudaMemsetAsync(constraint.p, 0, sizeof(i32) * constraint.n, ctx.stream));
+            parts.pop_back();
+            drop = false;
+        } else {
+            break;
+        }
+    }
+    if (st) {
+        st->levels = (i64)levels.size();
+        i64 t = 0;
+        for (auto* l : levels) t += l->nnz;
+        st->total_nnz = t;
+    }
+    if (levels.size() > 1) {
+        levels.pop_back();
+        parts.pop_back();
+    }
+    for (i64 i = (i64)levels.size() - 2; i >= 0; i--) {
+        const Graph<W>& c = *levels[i];
+        k_project<<<vgrid(ctx, c.n), 256, 0, ctx.stream>>>(c.n, parts[i].p, parts[i + 1].p);
+        PGGC_LAUNCH_CHECK();
+        generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        local_move<W>(ctx, c, ord, parts[i].p, rfd, false, false, nullptr, true, false, -1, &ms);
+    }
+    copy_d2d(ctx, labels_out, parts[0].p, top.n);
+    if (st) {
+        st->sweeps += ms.sweeps;
+        st->moves += ms.moves;
+    }
+}
+
+#define PGGC_INST_DRV(W)                                                                                              \
+    template void leiden_part<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, bool, bool, const i32*, u64, \
+                                 i32*, RunStats*);                                                                    \
+    template void louvain_part<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, bool, const i32*, i32*,     \
+                                  RunStats*);                                                                         \
+    template void make_cluster_state<W>(Context&, const Graph<W>&, int, double, ClusterState<Traits<W>::V>&);         \
+    template void default_vertex_weights<W>(Context&, Graph<W>&, int);
+PGGC_INST_DRV(i32)
+PGGC_INST_DRV(float)
+template void update_objective<i64>(Context&, ClusterState<i64>&);
+template void update_objective<double>(Context&, ClusterState<double>&);
+
+}  // namespace pggc

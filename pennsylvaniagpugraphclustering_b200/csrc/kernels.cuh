@@ -1,0 +1,144 @@
+// kernels.cuh -- host-side entry points of the kernel families and the device
+// state they share (weighted_graph, cluster_data, memory_store equivalents).
+#pragma once
+#include <memory>
+#include <vector>
+#include "scan.cuh"
+
+namespace pggc {
+
+// Vertices of degree above HUGE_DEG aggregate into global-memory tables; all
+// others use shared-memory tables.
+constexpr i64 HUGE_DEG = 4096;
+constexpr int SEL_TS_MAX = 8192;  // shared-memory table slots of the block kernels
+
+// ---------------------------------------------------------------------------
+// src/ordering.cpp:131-164 -- stable degree-bucket orderings
+// ---------------------------------------------------------------------------
+struct Ordering {
+    DBuf<i32> order1, order2, huge;
+    i64 n = 0;
+    i64 off_large = 0, off_large2 = 0, off_mid = 0, off_mid2 = 0;
+    i64 max_deg = 0, n_huge = 0;
+};
+void generate_orderings(Context& ctx, const i64* rowptr, i64 n, Ordering& o);
+
+// ---------------------------------------------------------------------------
+// weighted_graph (interface/weighted_graph.h:10-19), device resident
+// ---------------------------------------------------------------------------
+template <class W>
+struct Graph {
+    using V = typename Traits<W>::V;
+    i64 n = 0, nnz = 0;
+    bool uniform = true;  // unit edge weights; w is not allocated
+    DBuf<i64> rowptr;
+    DBuf<i32> col;
+    DBuf<W> w;
+    DBuf<V> vtx_w;
+    // borrowed (caller-owned) arrays take precedence over the owned ones
+    const i64* b_rowptr = nullptr;
+    const i32* b_col = nullptr;
+    const W* b_w = nullptr;
+    DGraph<W> view() const {
+        DGraph<W> g;
+        g.n = n;
+        g.nnz = nnz;
+        g.rowptr = b_rowptr ? b_rowptr : rowptr.p;
+        g.col = b_col ? b_col : col.p;
+        g.w = uniform ? nullptr : (b_w ? b_w : w.p);
+        g.vtx_w = vtx_w.p;
+        return g;
+    }
+};
+
+enum ObjKind { OBJ_MOD = 0, OBJ_WMOD = 1, OBJ_CPM = 2, OBJ_NLCC = 3, OBJ_LCC = 4 };
+
+// ---------------------------------------------------------------------------
+// cluster_data (interface/cluster_data.hpp:9-107): host scalars + device
+// total_deg with room for appended labels.
+// ---------------------------------------------------------------------------
+template <class V>
+struct ClusterState {
+    DBuf<V> total_deg;
+    i64 capacity = 0;
+    V uncut = 0;
+    i64 top_nnz = 0;
+    double obj = -1.0;
+    i64 label_count = 0;
+    double lambda = 1.0;
+    int kind = OBJ_LCC;
+    double inv_gdeg = 0.0, v_total = 0.0, g_deg = 0.0;
+    double get_objective() const {
+        switch (kind) {
+            case OBJ_MOD:
+            case OBJ_WMOD: return obj * inv_gdeg;
+            case OBJ_CPM: return obj + lambda * v_total;
+            case OBJ_NLCC: return obj / g_deg;
+            default: return obj;
+        }
+    }
+};
+
+// objective helpers (interface/cluster_data.hpp:76-87 and :109-181)
+template <class W>
+void make_cluster_state(Context& ctx, const Graph<W>& g, int kind, double mult, ClusterState<typename Traits<W>::V>& cs);
+template <class V>
+void update_objective(Context& ctx, ClusterState<V>& cs);
+template <class W>
+void default_vertex_weights(Context& ctx, Graph<W>& g, int objective);
+
+// ---------------------------------------------------------------------------
+// local move (src/local_mover.cpp)
+// ---------------------------------------------------------------------------
+struct MoveStats {
+    i64 sweeps = 0;
+    i64 moves = 0;
+};
+
+template <class W>
+void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_part,
+                ClusterState<typename Traits<W>::V>& best, bool is_initial, bool constrained, i32* constraint,
+                bool enable_sa, bool strict, int sweep_limit, MoveStats* stats);
+
+// one select pass (candidates_and_destinations) for parity tests
+template <class W>
+i64 select_pass(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* part,
+                const typename Traits<W>::V* pvals, ClusterState<typename Traits<W>::V>& cs, i32* dest, float* gain,
+                float filter_ratio, bool initial, bool constrained, const i32* constraint);
+
+// own-cluster weight of every vertex under `labels` (canonical sums)
+template <class W>
+void own_weights(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* labels, typename Traits<W>::V* out);
+
+// ---------------------------------------------------------------------------
+// contraction (src/contract.cpp:234-336) and Leiden refinement (src/leidenR.cpp)
+// ---------------------------------------------------------------------------
+template <class W>
+std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, const i32* vcmap, i64 nc);
+
+template <class W>
+void coarsen_vtx_w(Context& ctx, const Graph<W>& g, const i32* vcmap, Graph<W>& cg);
+
+template <class W>
+i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* constraint,
+                    const ClusterState<typename Traits<W>::V>& cs, u32 seed_pick, u32 seed_order, i32* vcmap_out);
+
+// ---------------------------------------------------------------------------
+// multilevel drivers (src/clustering_methods.cpp)
+// ---------------------------------------------------------------------------
+struct RunStats {
+    i64 levels = 0;
+    i64 total_nnz = 0;
+    i64 sweeps = 0;
+    i64 moves = 0;
+    i64 passes = 0;
+};
+
+template <class W>
+void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool plus, bool improve,
+                 const i32* input, u64 seed, i32* labels_out, RunStats* st);
+template <class W>
+void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool constrained,
+                  const i32* constraint, i32* labels_out, RunStats* st);
+
+}  // namespace pggc

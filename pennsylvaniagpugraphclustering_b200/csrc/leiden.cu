@@ -1,0 +1,552 @@
+// leiden.cu -- Leiden refinement, coarsen_leidenR<top,uniform>
+// (src/leidenR.cpp:41-500), for sm_100a.
+//
+//  * well-connectedness test, then a per-vertex neighbour pick inside the
+//    constraint cluster: first qualifying neighbour in cyclic order from a
+//    hashed start (unit weights; warp ballots find the first hit) or the
+//    weighted-random heaviest edge (max of |h/ORD_MAX| * val^4, ties to the
+//    last edge);
+//  * hashed vertex order, forest connected components by bounded pointer
+//    chasing (find_trees), order flip for the unassigned vertices;
+//  * gamma-connectivity: one stable LSD radix sort by (cluster, order, id)
+//    replaces the counting sort + sort_crs_matrix; prefix sums give cluster
+//    sizes and outward connectivity, two breakpoint passes and one break pass;
+//  * contiguous relabelling by a prefix sum.
+// The random picks use MurmurHash3_x86_32 (the hash behind Kokkos::pod_hash).
+#include "kernels.cuh"
+
+namespace pggc {
+
+template <class W>
+__global__ void k_well(DGraph<W> g, const i32* constraint, const typename Traits<W>::V* pv,
+                       const typename Traits<W>::V* td, float gamma, unsigned char* well) {
+    using V = typename Traits<W>::V;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < g.n; i += (i64)gridDim.x * blockDim.x) {
+        i32 c = constraint[i];
+        V wd = g.vtx_w[i];
+        well[i] = to_f(pv[i]) >= (gamma * to_f(wd)) * to_f(V(td[c] - wd)) ? 1 : 0;
+    }
+}
+
+template <class W>
+struct PickArgs {
+    DGraph<W> g;
+    const i32* constraint;
+    const unsigned char* well;
+    float gamma;
+    u32 seed;
+    i32* hn;
+};
+
+template <class W>
+__device__ __forceinline__ bool pick_ok_uniform(const PickArgs<W>& a, i32 i, i32 v, float multi) {
+    if (a.constraint[i] != a.constraint[v]) return false;
+    if (!a.well[v]) return false;
+    return 1.0f >= multi * to_f(a.g.vtx_w[v]);
+}
+
+// select random edge (src/leidenR.cpp:296-336), warp per vertex
+template <class W>
+__global__ void __launch_bounds__(256) k_pick_uniform_warp(PickArgs<W> a, const i32* list, i64 count) {
+    const int l = lane_id();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 x = gw; x < count; x += nw) {
+        i32 i = list[x];
+        i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        i64 width = e - b;
+        i32 jxs = (i32)murmur3_32(a.seed + (u32)i);
+        if (jxs % 1000 == 0 || !a.well[i] || width == 0) {
+            if (l == 0) a.hn[i] = i;
+            continue;
+        }
+        i64 jx = b + (i64)((u32)jxs % (u32)width);
+        float multi = a.gamma * to_f(a.g.vtx_w[i]);
+        i32 pick = i;
+        for (i64 off = 0; off < width; off += 32) {
+            i64 s = off + l;
+            bool q = false;
+            i32 v = -1;
+            if (s < width) {
+                i64 j = jx + s;
+                if (j >= e) j -= width;
+                v = a.g.col[j];
+                q = pick_ok_uniform(a, i, v, multi);
+            }
+            unsigned m = __ballot_sync(FULL, q);
+            if (m) {
+                pick = __shfl_sync(FULL, v, __ffs(m) - 1);
+                break;
+            }
+        }
+        if (l == 0) a.hn[i] = pick;
+    }
+}
+
+// the 1024-thread variant for degree >= 15000 (src/leidenR.cpp:342-393)
+template <class W>
+__global__ void __launch_bounds__(1024) k_pick_uniform_block(PickArgs<W> a, const i32* list, i64 count) {
+    __shared__ long long first;
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        i32 i = list[x];
+        i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        i64 width = e - b;
+        i32 jxs = (i32)murmur3_32(a.seed + (u32)i);
+        if (jxs % 1000 == 0 || !a.well[i] || width == 0) {
+            if (threadIdx.x == 0) a.hn[i] = i;
+            continue;
+        }
+        i64 jx = b + (i64)((u32)jxs % (u32)width);
+        float multi = a.gamma * to_f(a.g.vtx_w[i]);
+        if (threadIdx.x == 0) first = width;
+        __syncthreads();
+        for (i64 off = 0; off < width; off += 1024) {
+            i64 s = off + threadIdx.x;
+            if (s < width) {
+                i64 j = jx + s;
+                if (j >= e) j -= width;
+                if (pick_ok_uniform(a, i, a.g.col[j], multi)) atomicMin(&first, (long long)s);
+            }
+            __syncthreads();
+            if (first < width) break;
+        }
+        if (threadIdx.x == 0) {
+            if (first < width) {
+                i64 j = jx + first;
+                if (j >= e) j -= width;
+                a.hn[i] = a.g.col[j];
+            } else {
+                a.hn[i] = i;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// select heaviest edge (src/leidenR.cpp:400-474): max sample, ties -> last edge
+__device__ __forceinline__ bool sample_better(float s, i64 j, float bs, i64 bj) {
+    return s > bs || (s == bs && j > bj);
+}
+
+template <class W>
+__device__ __forceinline__ void heavy_eval(const PickArgs<W>& a, i32 i, i64 j, float multi, float& bs, i64& bj) {
+    i32 v = a.g.col[j];
+    if (a.constraint[i] != a.constraint[v]) return;
+    if (!a.well[v]) return;
+    float val = (float)a.g.wgt(j) - multi * to_f(a.g.vtx_w[v]);
+    if (val >= 0.0f) {
+        float sample = fabsf((float)murmur3_32(a.seed + (u32)(u64)j) / (float)ORD_MAX);
+        float v2 = val * val;
+        sample = sample * (v2 * v2);
+        if (sample >= 0.0f && sample_better(sample, j, bs, bj)) {
+            bs = sample;
+            bj = j;
+        }
+    }
+}
+
+template <class W>
+__global__ void __launch_bounds__(256) k_pick_heavy_warp(PickArgs<W> a, const i32* list, i64 count) {
+    const int l = lane_id();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 x = gw; x < count; x += nw) {
+        i32 i = list[x];
+        i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        u32 h = murmur3_32(a.seed + (u32)i);
+        if (h % 10000u == 0 || !a.well[i]) {
+            if (l == 0) a.hn[i] = i;
+            continue;
+        }
+        float multi = a.gamma * to_f(a.g.vtx_w[i]);
+        float bs = -1.0f;
+        i64 bj = -1;
+        for (i64 j = b + l; j < e; j += 32) heavy_eval(a, i, j, multi, bs, bj);
+        for (int d = 16; d >= 1; d >>= 1) {
+            float os = __shfl_xor_sync(FULL, bs, d);
+            i64 oj = __shfl_xor_sync(FULL, bj, d);
+            if (sample_better(os, oj, bs, bj)) {
+                bs = os;
+                bj = oj;
+            }
+        }
+        if (l == 0) a.hn[i] = bj >= b ? a.g.col[bj] : i;
+    }
+}
+
+template <class W>
+__global__ void __launch_bounds__(1024) k_pick_heavy_block(PickArgs<W> a, const i32* list, i64 count) {
+    __shared__ float ws[32];
+    __shared__ i64 wj[32];
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        i32 i = list[x];
+        i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        u32 h = murmur3_32(a.seed + (u32)i);
+        if (h % 10000u == 0 || !a.well[i]) {
+            if (threadIdx.x == 0) a.hn[i] = i;
+            continue;
+        }
+        float multi = a.gamma * to_f(a.g.vtx_w[i]);
+        float bs = -1.0f;
+        i64 bj = -1;
+        for (i64 j = b + threadIdx.x; j < e; j += 1024) heavy_eval(a, i, j, multi, bs, bj);
+        for (int d = 16; d >= 1; d >>= 1) {
+            float os = __shfl_xor_sync(FULL, bs, d);
+            i64 oj = __shfl_xor_sync(FULL, bj, d);
+            if (sample_better(os, oj, bs, bj)) {
+                bs = os;
+                bj = oj;
+            }
+        }
+        if (lane_id() == 0) {
+            ws[threadIdx.x >> 5] = bs;
+            wj[threadIdx.x >> 5] = bj;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            bs = ws[threadIdx.x];
+            bj = wj[threadIdx.x];
+            for (int d = 16; d >= 1; d >>= 1) {
+                float os = __shfl_xor_sync(FULL, bs, d);
+                i64 oj = __shfl_xor_sync(FULL, bj, d);
+                if (sample_better(os, oj, bs, bj)) {
+                    bs = os;
+                    bj = oj;
+                }
+            }
+            if (threadIdx.x == 0) a.hn[i] = bj >= b ? a.g.col[bj] : i;
+        }
+        __syncthreads();
+    }
+}
+
+// set order + unselect equal order edges (src/leidenR.cpp:482-494)
+__global__ void k_set_order(i64 n, u32 seed, i32* order) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        i32 o = (i32)murmur3_32((u32)i + seed);
+        order[i] = abs(o % SPLIT);
+    }
+}
+__global__ void k_unselect(i64 n, const i32* order, i32* hn) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        i32 h = hn[i];
+        if (order[i] == order[h]) hn[i] = (i32)i;
+    }
+}
+
+// find_trees (src/leidenR.cpp:213-260); pointer chasing bounded by n steps
+__global__ void k_trees_part1(i64 n, const i32* hn, const i32* order, i32* vcmap, int* err) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        i32 now = (i32)i, then = hn[i];
+        if (now == then) {
+            vcmap[i] = (i32)i;
+            continue;
+        }
+        i64 steps = 0;
+        while (order[now] > order[then]) {
+            now = then;
+            then = hn[then];
+            if (++steps > n) {
+                atomicExch(err, (int)DEV_ERR_CHASE);
+                break;
+            }
+        }
+        if (now != (i32)i) {
+            vcmap[i] = now;
+            vcmap[now] = now;
+        }
+    }
+}
+__global__ void k_trees_flip(i64 n, const i32* vcmap, i32* order) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        if (vcmap[i] == ORD_MAX) order[i] = 2 * SPLIT - order[i];
+}
+__global__ void k_trees_part2(i64 n, const i32* hn, const i32* order, i32* vcmap, int* err) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        volatile i32* vc = vcmap;
+        if (vc[i] != ORD_MAX) continue;
+        i32 now = (i32)i, then = hn[i];
+        i64 steps = 0;
+        while (vc[now] == ORD_MAX && order[now] > order[then]) {
+            now = then;
+            then = hn[then];
+            if (++steps > n) {
+                atomicExch(err, (int)DEV_ERR_CHASE);
+                break;
+            }
+        }
+        vc[i] = vc[now];
+    }
+}
+
+// ---- ensure_gamma_connectivity (src/leidenR.cpp:41-187) --------------------
+__global__ void k_sort_keys(i64 n, const i32* vcmap, const i32* order, u64* keys, i32* ids) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        keys[i] = ((u64)(u32)vcmap[i] << 31) | (u64)(u32)order[i];
+        ids[i] = (i32)i;
+    }
+}
+__global__ void k_hist(i64 n, const i32* lab, i64* cnt) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        ::atomicAdd((unsigned long long*)&cnt[lab[i]], 1ull);
+}
+
+template <class V>
+struct TsIn;
+template <>
+struct TsIn<i64> {
+    const i32* ids;
+    const i64* vw;
+    i64 n;
+    __device__ i64 operator()(i64 x) const { return x < n ? vw[ids[x]] : 0; }
+};
+template <>
+struct TsIn<double> {
+    const i32* ids;
+    const double* vw;
+    i64 n;
+    __device__ double operator()(i64 x) const { return vw[ids[x]]; }
+};
+
+template <class W>
+__device__ __forceinline__ typename Traits<W>::V inner_term(const DGraph<W>& g, const i32* vcmap, const i32* order,
+                                                            i32 i, i64 j) {
+    using V = typename Traits<W>::V;
+    i32 v = g.col[j];
+    return (vcmap[i] == vcmap[v] && order[v] < order[i]) ? V(g.wgt(j)) : V(0);
+}
+
+template <class W>
+__global__ void __launch_bounds__(256) k_inner_warp(DGraph<W> g, const i32* list, i64 count, const i32* vcmap,
+                                                    const i32* order, typename Traits<W>::V* inner) {
+    using V = typename Traits<W>::V;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 x = gw; x < count; x += nw) {
+        i32 i = list[x];
+        V r = VSum<V>::warp(g.rowptr[i], g.rowptr[i + 1], [&](i64 j) { return inner_term(g, vcmap, order, i, j); });
+        if (lane_id() == 0) inner[i] = r;
+    }
+}
+
+template <class W>
+__global__ void __launch_bounds__(1024) k_inner_block(DGraph<W> g, const i32* list, i64 count, const i32* vcmap,
+                                                      const i32* order, typename Traits<W>::V* inner) {
+    using V = typename Traits<W>::V;
+    __shared__ double red[32];
+    __shared__ unsigned long long acc;
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        i32 i = list[x];
+        i64 b = g.rowptr[i], e = g.rowptr[i + 1];
+        V r;
+        if constexpr (std::is_same<V, double>::value) {
+            r = block1024_canon_sum(b, e, [&](i64 j) { return inner_term(g, vcmap, order, i, j); }, red);
+        } else {
+            if (threadIdx.x == 0) acc = 0;
+            __syncthreads();
+            i64 s = 0;
+            for (i64 j = b + threadIdx.x; j < e; j += 1024) s += inner_term(g, vcmap, order, i, j);
+            s = warp_sum_i64(s);
+            if (lane_id() == 0) ::atomicAdd(&acc, (unsigned long long)s);
+            __syncthreads();
+            r = (i64)acc;
+        }
+        if (threadIdx.x == 0) inner[i] = r;
+        __syncthreads();
+    }
+}
+
+template <class W>
+struct GammaArgs {
+    using V = typename Traits<W>::V;
+    i64 n;
+    const i32* ids;
+    const i32* vcmap;
+    const i64* row_map;
+    const V* ts;
+    const V* inner;
+    const V* oc;
+    const V* vw;
+    const V* td;
+    const i32* constraint;
+    float gamma;
+    long long* breakers;
+};
+
+template <class W>
+__global__ void k_break_part1(GammaArgs<W> a) {
+    using V = typename Traits<W>::V;
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < a.n; x += (i64)gridDim.x * blockDim.x) {
+        i32 i = a.ids[x];
+        i32 c = a.vcmap[i];
+        i64 cb = a.row_map[c];
+        V prev = a.ts[x] - a.ts[cb];
+        if (to_f(a.inner[i]) < (a.gamma * to_f(a.vw[i])) * to_f(prev)) atomicMin(&a.breakers[c], (long long)x);
+    }
+}
+template <class W>
+__global__ void k_break_part2(GammaArgs<W> a) {
+    using V = typename Traits<W>::V;
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < a.n; x += (i64)gridDim.x * blockDim.x) {
+        i32 i = a.ids[x];
+        i32 c = a.vcmap[i];
+        i64 cb = a.row_map[c];
+        V curr_size = (a.ts[x] + a.vw[i]) - a.ts[cb];
+        V other = a.td[a.constraint[i]] - curr_size;
+        V outer = a.oc[i];
+        if (cb > 0) outer = outer - a.oc[a.ids[cb - 1]];
+        if (to_f(outer) < (a.gamma * to_f(curr_size)) * to_f(other)) atomicMin(&a.breakers[c], (long long)(x + 1));
+    }
+}
+__global__ void k_break_apply(i64 n, const i32* ids, const long long* breakers, i32* vcmap) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n; x += (i64)gridDim.x * blockDim.x) {
+        i32 i = ids[x];
+        i32 c = vcmap[i];
+        if (x >= breakers[c]) vcmap[i] = i;
+    }
+}
+
+template <class V>
+struct OcInI {
+    const i32* ids;
+    const V* pv;
+    const V* inner;
+    __device__ i64 operator()(i64 x) const {
+        i32 i = ids[x];
+        return pv[i] - 2 * inner[i];
+    }
+};
+struct OcEpiI {
+    const i32* ids;
+    i64* oc;
+    __device__ void operator()(i64 x, i64 excl, i64 v) const { oc[ids[x]] = excl + v; }
+};
+struct OcInD {
+    const i32* ids;
+    const double* pv;
+    const double* inner;
+    __device__ double operator()(i64 x) const {
+        i32 i = ids[x];
+        return pv[i] - 2.0 * inner[i];
+    }
+};
+__global__ void k_scatter_by_ids(i64 n, const i32* ids, const double* in, double* out) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n; x += (i64)gridDim.x * blockDim.x) out[ids[x]] = in[x];
+}
+__global__ void k_shift_excl(i64 n, const double* inc, double* ts) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n; x += (i64)gridDim.x * blockDim.x)
+        ts[x] = x == 0 ? 0.0 : inc[x - 1];
+}
+
+// contigitize_clusters (src/leidenR.cpp:190-210)
+struct RootFlag {
+    const i32* vcmap;
+    __device__ i64 operator()(i64 u) const { return vcmap[u] == (i32)u ? 1 : 0; }
+};
+struct RootEpi {
+    i32* newid;
+    __device__ void operator()(i64 u, i64 excl, i64 v) const {
+        if (v) newid[u] = (i32)excl;
+    }
+};
+__global__ void k_contig_apply(i64 n, const i32* vcmap, const i32* newid, i32* out) {
+    for (i64 u = blockIdx.x * (i64)blockDim.x + threadIdx.x; u < n; u += (i64)gridDim.x * blockDim.x)
+        out[u] = newid[vcmap[u]];
+}
+
+template <class W>
+i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* constraint,
+                    const ClusterState<typename Traits<W>::V>& cs, u32 seed_pick, u32 seed_order, i32* vcmap_out) {
+    using V = typename Traits<W>::V;
+    const i64 n = g.n;
+    if (n == 0) return 0;
+    auto gv = g.view();
+    const float gamma = (float)cs.lambda;
+    const int grid = (int)std::min<i64>(ceil_div(n, 256), (i64)ctx.num_sms * 16);
+    const i64 nsmall = ord.off_large2, nmass = n - ord.off_large2;
+    const i32* small_list = ord.order1.p;
+    const i32* mass_list = ord.order1.p + ord.off_large2;
+    const int gw = (int)std::min<i64>(ceil_div(std::max<i64>(nsmall, 1), 8), (i64)ctx.num_sms * 16);
+    const int gb = (int)std::min<i64>(std::max<i64>(nmass, 1), (i64)ctx.num_sms * 2);
+
+    DBuf<V> pv(ctx, n);
+    own_weights<W>(ctx, g, ord, constraint, pv.p);
+    DBuf<unsigned char> well(ctx, n);
+    k_well<W><<<grid, 256, 0, ctx.stream>>>(gv, constraint, pv.p, cs.total_deg.p, gamma, well.p);
+    PGGC_LAUNCH_CHECK();
+    DBuf<i32> hn(ctx, n), order(ctx, n), vcmap(ctx, n);
+    PickArgs<W> pa{gv, constraint, well.p, gamma, seed_pick, hn.p};
+    if (g.uniform) {
+        if (nsmall > 0) k_pick_uniform_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list, nsmall);
+        if (nmass > 0) k_pick_uniform_block<W><<<gb, 1024, 0, ctx.stream>>>(pa, mass_list, nmass);
+    } else {
+        if (nsmall > 0) k_pick_heavy_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list, nsmall);
+        if (nmass > 0) k_pick_heavy_block<W><<<gb, 1024, 0, ctx.stream>>>(pa, mass_list, nmass);
+    }
+    PGGC_LAUNCH_CHECK();
+    k_set_order<<<grid, 256, 0, ctx.stream>>>(n, seed_order, order.p);
+    k_unselect<<<grid, 256, 0, ctx.stream>>>(n, order.p, hn.p);
+    fill<i32>(ctx, vcmap.p, n, ORD_MAX);
+    k_trees_part1<<<grid, 256, 0, ctx.stream>>>(n, hn.p, order.p, vcmap.p, ctx.d_err);
+    k_trees_flip<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, order.p);
+    k_trees_part2<<<grid, 256, 0, ctx.stream>>>(n, hn.p, order.p, vcmap.p, ctx.d_err);
+    PGGC_LAUNCH_CHECK();
+
+    // --- gamma connectivity
+    DBuf<u64> keys(ctx, n), keys2(ctx, n);
+    DBuf<i32> ids(ctx, n), ids2(ctx, n);
+    k_sort_keys<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, order.p, keys.p, ids.p);
+    PGGC_LAUNCH_CHECK();
+    radix_sort_pairs<i32>(ctx, keys.p, ids.p, n, 0, 31 + bits_for((u64)(n - 1)), keys2.p, ids2.p);
+    DBuf<i64> cnt(ctx, n + 1), row_map(ctx, n + 1);
+    PGGC_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(i64) * (n + 1), ctx.stream));
+    k_hist<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, cnt.p);
+    PGGC_LAUNCH_CHECK();
+    scan_apply(ctx, ArrIn{cnt.p}, ArrOutExcl{row_map.p}, n + 1, nullptr, nullptr);
+    DBuf<V> ts(ctx, n), inner(ctx, n), oc(ctx, n);
+    if constexpr (std::is_same<V, i64>::value) {
+        scan_apply(ctx, TsIn<i64>{ids.p, g.vtx_w.p, n}, ArrOutExcl{ts.p}, n, nullptr, nullptr);
+    } else {
+        DBuf<double> inc(ctx, n);
+        det_scan(ctx, TsIn<double>{ids.p, g.vtx_w.p, n}, inc.p, n);
+        k_shift_excl<<<grid, 256, 0, ctx.stream>>>(n, inc.p, ts.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    if (nsmall > 0) k_inner_warp<W><<<gw, 256, 0, ctx.stream>>>(gv, small_list, nsmall, vcmap.p, order.p, inner.p);
+    if (nmass > 0) k_inner_block<W><<<gb, 1024, 0, ctx.stream>>>(gv, mass_list, nmass, vcmap.p, order.p, inner.p);
+    PGGC_LAUNCH_CHECK();
+    DBuf<long long> breakers(ctx, n);
+    fill<long long>(ctx, breakers.p, n, (long long)n);
+    GammaArgs<W> ga{n, ids.p, vcmap.p, row_map.p, ts.p, inner.p, oc.p, g.vtx_w.p, cs.total_deg.p, constraint, gamma,
+                    breakers.p};
+    k_break_part1<W><<<grid, 256, 0, ctx.stream>>>(ga);
+    PGGC_LAUNCH_CHECK();
+    if constexpr (std::is_same<V, i64>::value) {
+        scan_apply(ctx, OcInI<i64>{ids.p, pv.p, inner.p}, OcEpiI{ids.p, oc.p}, n, nullptr, nullptr);
+    } else {
+        DBuf<double> inc(ctx, n);
+        det_scan(ctx, OcInD{ids.p, pv.p, inner.p}, inc.p, n);
+        k_scatter_by_ids<<<grid, 256, 0, ctx.stream>>>(n, ids.p, inc.p, oc.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    k_break_part2<W><<<grid, 256, 0, ctx.stream>>>(ga);
+    k_break_apply<<<grid, 256, 0, ctx.stream>>>(n, ids.p, breakers.p, vcmap.p);
+    PGGC_LAUNCH_CHECK();
+
+    // --- contigitize
+    DBuf<i32> newid(ctx, n);
+    DBuf<i64> tot(ctx, 1);
+    scan_apply(ctx, RootFlag{vcmap.p}, RootEpi{newid.p}, n, nullptr, tot.p);
+    k_contig_apply<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, newid.p, vcmap_out);
+    PGGC_LAUNCH_CHECK();
+    i64 nc = ctx.read1(tot.p);
+    ctx.check_device_error();
+    return nc;
+}
+
+template i64 coarsen_leidenR<i32>(Context&, const Graph<i32>&, const Ordering&, const i32*, const ClusterState<i64>&, u32,
+                                  u32, i32*);
+template i64 coarsen_leidenR<float>(Context&, const Graph<float>&, const Ordering&, const i32*,
+                                    const ClusterState<double>&, u32, u32, i32*);
+
+}  // namespace pggc

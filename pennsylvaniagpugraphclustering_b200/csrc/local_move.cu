@@ -1,0 +1,1216 @@
+// local_move.cu -- the synchronous parallel local-move sweep
+// (src/local_mover.cpp:100-1483) rebuilt for sm_100a.
+//
+// Design (vs. the reference's persistent per-vertex hash tables):
+//  * No conn tables are kept between sweeps.  The DeltaQ argmax aggregates each
+//    evaluated vertex's neighbour-cluster weights on the fly: a warp per vertex
+//    (degree < 128) pre-aggregates each 32-edge chunk with __match_any_sync and
+//    either reduces it directly (degree <= 32) or inserts group sums into a
+//    per-warp shared-memory table; a 256-thread block per vertex with a
+//    shared-memory table (degree <= 4096); global-memory tables for larger
+//    degrees.  Aggregated sums are exact, so the result equals the reference's
+//    table contents; ties go to the smallest cluster id.
+//  * The own-cluster weights (pvals) are recomputed exactly for the vertices
+//    whose neighbourhood changed, which is the set whose dest cache the
+//    reference invalidates (moved vertices and their neighbours).
+//  * Candidate / move lists are order-preserving compactions of order1, so new
+//    cluster ids and the strict prefix follow the reference's move order.
+//  * One host round trip per sweep (candidate and move counts); everything else
+//    reads counts from device memory.
+#include "kernels.cuh"
+
+namespace pggc {
+
+template <class V>
+struct LMScalars {
+    i64 num_cand, split, num_moves, num_new, num_avail, avail_k;
+    i64 label_count, best_label_count;
+    V uncut, best_uncut, last_pval, pval_sum;
+    i64 sumsq_i;
+    double sumsq_d;
+    double obj, best_obj;
+    int improved;
+    int pad[3];
+};
+
+__device__ __forceinline__ void vatomic_add(i64* a, i64 x) { ::atomicAdd((unsigned long long*)a, (unsigned long long)x); }
+__device__ __forceinline__ void vatomic_add(double* a, double x) { ::atomicAdd(a, x); }
+
+struct Best {
+    float jc;
+    i32 c;
+};
+__device__ __forceinline__ bool better(float jc, i32 c, const Best& b) { return jc > b.jc || (jc == b.jc && c < b.c); }
+__device__ __forceinline__ Best none_best() { return Best{-INFINITY, 2147483647}; }
+__device__ __forceinline__ void warp_best(Best& b) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+        float oj = __shfl_xor_sync(FULL, b.jc, d);
+        i32 oc = __shfl_xor_sync(FULL, b.c, d);
+        if (better(oj, oc, b)) b = Best{oj, oc};
+    }
+}
+
+template <class W>
+struct SelArgs {
+    using V = typename Traits<W>::V;
+    DGraph<W> g;
+    const i32* part;
+    i32* dest;
+    float* gain;
+    const V* pvals;
+    const V* td;
+    const i32* constraint;
+    const i64* label_count;  // device
+    float pm;
+    float fr;
+    int initial;
+    int* err;
+};
+
+struct VCtx {
+    i32 p;
+    float multi, p_conn, thr;
+};
+
+template <class W>
+__device__ __forceinline__ VCtx sel_prologue(const SelArgs<W>& a, i32 i) {
+    using V = typename Traits<W>::V;
+    VCtx v;
+    V w = a.g.vtx_w[i];
+    v.multi = to_f(w) * a.pm;
+    v.p = a.part[i];
+    v.p_conn = to_f(a.pvals[i]) - to_f(V(a.td[v.p] - w)) * v.multi;
+    v.thr = v.p_conn < 0.0f ? 0.0f : (float)((double)v.p_conn * (1.0 - (double)a.fr));
+    return v;
+}
+
+template <class W, bool CON>
+__device__ __forceinline__ void sel_eval(const SelArgs<W>& a, const VCtx& vc, i32 c, typename Traits<W>::V jv,
+                                         Best& b) {
+    using V = typename Traits<W>::V;
+    if (!(jv > V(0))) return;
+    float f = to_f(jv);
+    if (!(f >= vc.thr)) return;
+    if (CON && a.constraint[c] != a.constraint[vc.p]) return;
+    float jc = f - to_f(a.td[c]) * vc.multi;
+    if (jc >= vc.thr && better(jc, c, b)) b = Best{jc, c};
+}
+
+template <class W>
+__device__ __forceinline__ void sel_finish(const SelArgs<W>& a, i32 i, const VCtx& vc, const Best& b) {
+    if (b.c != 2147483647) {
+        a.dest[i] = b.c;
+        a.gain[i] = b.jc - vc.p_conn;
+    } else if (vc.p_conn < 0.0f) {
+        a.dest[i] = NEW_PART;
+        a.gain[i] = -vc.p_conn;
+    } else {
+        a.dest[i] = NO_MOVE;
+        a.gain[i] = OBJ_MIN;
+    }
+}
+
+// Sum of `val` over the lanes of `peers` (lane order), valid at the group leader.
+template <class V>
+__device__ __forceinline__ V group_sum(unsigned peers, V val, bool leader) {
+    int size = __popc(peers);
+    int maxsize = __reduce_max_sync(FULL, (unsigned)size);
+    V s = V(0);
+    unsigned rem = peers;
+    const int l = lane_id();
+    for (int r = 0; r < maxsize; r++) {
+        int src = l;
+        bool take = leader && rem;
+        if (take) {
+            src = __ffs(rem) - 1;
+            rem &= rem - 1;
+        }
+        V x = __shfl_sync(FULL, val, src);
+        if (take) s = s + x;
+    }
+    return s;
+}
+
+template <class V>
+__device__ __forceinline__ void table_add(i32* keys, V* vals, u32 mask, i32 c, V x, int* err) {
+    u32 s = xorshift32((u32)c) & mask;
+    volatile i32* vk = keys;
+    for (u32 probe = 0; probe <= mask; probe++) {
+        i32 k = vk[s];
+        if (k == c) {
+            vatomic_add(&vals[s], x);
+            return;
+        }
+        if (k == -1) {
+            i32 old = atomicCAS(&keys[s], -1, c);
+            if (old == -1 || old == c) {
+                vatomic_add(&vals[s], x);
+                return;
+            }
+        }
+        s = (s + 1) & mask;
+    }
+    atomicExch(err, (int)DEV_ERR_PROBE);
+}
+
+// Aggregates one 32-edge chunk (edges j = base + lane, valid if < e) into the
+// table, skipping the vertex's own cluster.
+template <class W>
+__device__ __forceinline__ void chunk_to_table(const SelArgs<W>& a, const VCtx& vc, i64 j, i64 e, i32* keys,
+                                               typename Traits<W>::V* vals, u32 mask) {
+    using V = typename Traits<W>::V;
+    bool valid = j < e;
+    i32 c = valid ? a.part[a.g.col[j]] : -1;
+    V wv = valid ? V(a.g.wgt(j)) : V(0);
+    bool keep = valid && c != vc.p;
+    i32 key = keep ? c : (i32)(0x80000000u | lane_id());
+    unsigned peers = __match_any_sync(FULL, key);
+    bool leader = keep && ((peers & lanemask_lt()) == 0);
+    V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
+    if (leader) table_add(keys, vals, mask, c, s, a.err);
+}
+
+// ---- warp per vertex, degree < 128 (order1 bucket 0) ----------------------
+constexpr int SELW_WARPS = 8;
+constexpr int SELW_T = 256;
+
+template <class W, bool CON>
+__global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, const i32* list, i64 count) {
+    using V = typename Traits<W>::V;
+    __shared__ i32 tk[SELW_WARPS][SELW_T];
+    __shared__ V tv[SELW_WARPS][SELW_T];
+    const int l = lane_id(), w = threadIdx.x >> 5;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 x = gw; x < count; x += nw) {
+        i32 i = list[x];
+        if (a.dest[i] == NO_MOVE) continue;
+        VCtx vc = sel_prologue(a, i);
+        i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        Best best = none_best();
+        if (a.initial) {
+            for (i64 j = b + l; j < e; j += 32) sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
+        } else if (e - b <= 32) {
+            i64 j = b + l;
+            bool valid = j < e;
+            i32 c = valid ? a.part[a.g.col[j]] : -1;
+            V wv = valid ? V(a.g.wgt(j)) : V(0);
+            bool keep = valid && c != vc.p;
+            i32 key = keep ? c : (i32)(0x80000000u | l);
+            unsigned peers = __match_any_sync(FULL, key);
+            bool leader = keep && ((peers & lanemask_lt()) == 0);
+            V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
+            if (leader) sel_eval<W, CON>(a, vc, c, s, best);
+        } else {
+            u32 T = next_pow2_u32((u32)(2 * (e - b)));
+            i32* keys = tk[w];
+            V* vals = tv[w];
+            for (u32 s = l; s < T; s += 32) {
+                keys[s] = -1;
+                vals[s] = V(0);
+            }
+            __syncwarp();
+            for (i64 j = b + l; j - l < e; j += 32) chunk_to_table(a, vc, j, e, keys, vals, T - 1);
+            __syncwarp();
+            for (u32 s = l; s < T; s += 32) {
+                i32 c = keys[s];
+                if (c != -1) sel_eval<W, CON>(a, vc, c, vals[s], best);
+            }
+            __syncwarp();
+        }
+        warp_best(best);
+        if (l == 0) sel_finish(a, i, vc, best);
+    }
+}
+
+// ---- block per vertex (256 threads), shared or global table ----------------
+template <class W, bool CON, bool GLOBAL>
+__global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* list, i64 count, i32* gkeys,
+                                                      typename Traits<W>::V* gvals, i64 gcap) {
+    using V = typename Traits<W>::V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Best wb[8];
+    V* svals = (V*)smem_raw;
+    i32* skeys = (i32*)(smem_raw + sizeof(V) * SEL_TS_MAX);
+    const int l = lane_id(), w = threadIdx.x >> 5;
+    i32* keys = GLOBAL ? gkeys + (i64)blockIdx.x * gcap : skeys;
+    V* vals = GLOBAL ? gvals + (i64)blockIdx.x * gcap : svals;
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        i32 i = list[x];
+        i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        if (!GLOBAL && e - b > HUGE_DEG) continue;
+        if (a.dest[i] == NO_MOVE) continue;
+        VCtx vc = sel_prologue(a, i);
+        Best best = none_best();
+        if (a.initial) {
+            for (i64 j = b + threadIdx.x; j < e; j += 256) sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
+        } else {
+            i64 U = min(e - b, *a.label_count);
+            u32 T = next_pow2_u32((u32)(2 * U));
+            for (u32 s = threadIdx.x; s < T; s += 256) {
+                keys[s] = -1;
+                vals[s] = V(0);
+            }
+            __syncthreads();
+            for (i64 j = b + (i64)w * 32 + l; j - l < e; j += 256) chunk_to_table(a, vc, j, e, keys, vals, T - 1);
+            __syncthreads();
+            for (u32 s = threadIdx.x; s < T; s += 256) {
+                i32 c = keys[s];
+                if (c != -1) sel_eval<W, CON>(a, vc, c, vals[s], best);
+            }
+        }
+        warp_best(best);
+        if (l == 0) wb[w] = best;
+        __syncthreads();
+        if (w == 0) {
+            best = l < 8 ? wb[l] : none_best();
+            warp_best(best);
+            if (l == 0) sel_finish(a, i, vc, best);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// own-cluster weights (pvals)
+// ---------------------------------------------------------------------------
+template <class W>
+__device__ __forceinline__ typename Traits<W>::V own_warp(const DGraph<W>& g, const i32* lab, i32 i) {
+    using V = typename Traits<W>::V;
+    i64 b = g.rowptr[i], e = g.rowptr[i + 1];
+    i32 li = lab[i];
+    return VSum<V>::warp(b, e, [&](i64 j) -> V { return lab[g.col[j]] == li ? V(g.wgt(j)) : V(0); });
+}
+
+template <class W>
+__device__ __forceinline__ typename Traits<W>::V own_block1024(const DGraph<W>& g, const i32* lab, i32 i, double* red) {
+    using V = typename Traits<W>::V;
+    i64 b = g.rowptr[i], e = g.rowptr[i + 1];
+    i32 li = lab[i];
+    if constexpr (std::is_same<V, double>::value) {
+        return block1024_canon_sum(b, e, [&](i64 j) -> double { return lab[g.col[j]] == li ? (double)g.wgt(j) : 0.0; },
+                                   red);
+    } else {
+        __shared__ unsigned long long acc;
+        if (threadIdx.x == 0) acc = 0;
+        __syncthreads();
+        i64 s = 0;
+        for (i64 j = b + threadIdx.x; j < e; j += 1024)
+            if (lab[g.col[j]] == li) s += g.wgt(j);
+        s = warp_sum_i64(s);
+        if (lane_id() == 0) ::atomicAdd(&acc, (unsigned long long)s);
+        __syncthreads();
+        i64 r = (i64)acc;
+        __syncthreads();
+        return r;
+    }
+}
+
+// mode 0: every vertex (natural order, skipping massive ones)
+// mode 1: only flagged vertices; also resets dest to NULL_PART and clears the flag
+template <class W>
+__global__ void __launch_bounds__(256) k_own_warp(DGraph<W> g, const i32* lab, typename Traits<W>::V* out, int mode,
+                                                  unsigned char* flags, i32* dest) {
+    const int l = lane_id();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 base = gw * 32; base < g.n; base += nw * 32) {
+        i64 v = base + l;
+        bool want = false;
+        if (v < g.n) {
+            bool small = (g.rowptr[v + 1] - g.rowptr[v]) < MASSIVE_CUTOFF;
+            want = small && (mode == 0 || flags[v]);
+        }
+        unsigned m = __ballot_sync(FULL, want);
+        while (m) {
+            int src = __ffs(m) - 1;
+            m &= m - 1;
+            i32 i = (i32)(base + src);
+            auto r = own_warp(g, lab, i);
+            if (l == 0) {
+                out[i] = r;
+                if (mode == 1) {
+                    dest[i] = NULL_PART;
+                    flags[i] = 0;
+                }
+            }
+        }
+    }
+}
+
+template <class W>
+__global__ void __launch_bounds__(1024) k_own_massive(DGraph<W> g, const i32* lab, typename Traits<W>::V* out,
+                                                      const i32* list, i64 count, int mode, unsigned char* flags,
+                                                      i32* dest) {
+    __shared__ double red[32];
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        i32 i = list[x];
+        if (mode == 1 && !flags[i]) continue;
+        auto r = own_block1024(g, lab, i, red);
+        if (threadIdx.x == 0) {
+            out[i] = r;
+            if (mode == 1) {
+                dest[i] = NULL_PART;
+                flags[i] = 0;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <class W>
+void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* lab,
+                      typename Traits<W>::V* out, int mode, unsigned char* flags, i32* dest) {
+    auto gv = g.view();
+    if (g.n == 0) return;
+    int grid = (int)std::min<i64>(ceil_div(ceil_div(g.n, 32), 8), (i64)ctx.num_sms * 16);
+    k_own_warp<W><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, mode, flags, dest);
+    PGGC_LAUNCH_CHECK();
+    i64 nm = g.n - ord.off_large2;
+    if (nm > 0) {
+        int gb = (int)std::min<i64>(nm, (i64)ctx.num_sms * 2);
+        k_own_massive<W><<<gb, 1024, 0, ctx.stream>>>(gv, lab, out, ord.order1.p + ord.off_large2, nm, mode, flags,
+                                                       dest);
+        PGGC_LAUNCH_CHECK();
+    }
+}
+
+template <class W>
+void own_weights(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* labels, typename Traits<W>::V* out) {
+    own_weights_impl<W>(ctx, g, ord, labels, out, 0, nullptr, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// afterburner (src/local_mover.cpp:280-433)
+// ---------------------------------------------------------------------------
+template <class W>
+struct ABArgs {
+    using V = typename Traits<W>::V;
+    DGraph<W> g;
+    const i32* part;
+    const i32* dest;
+    const float* gain;
+    float pm;
+    const i32* cand;
+    unsigned char* keep;
+    const LMScalars<V>* sc;
+};
+
+template <class W>
+__device__ __forceinline__ double ab_term(const ABArgs<W>& a, i64 j, i32 p, i32 best, float multi, float igain,
+                                          i32 hi) {
+    i32 v = a.g.col[j];
+    float vgain = a.gain[v];
+    float d = vgain - igain;
+    if (d >= AFTERBURNER_EPS || (fabsf(d) < AFTERBURNER_EPS && (i32)xorshift32((u32)v) < hi)) {
+        float q = (float)a.g.wgt(j) - multi * to_f(a.g.vtx_w[v]);
+        int coef = 0;
+        i32 vp = a.dest[v];
+        if (vp == p) coef--;
+        if (vp == best && best != NEW_PART) coef++;
+        vp = a.part[v];
+        if (vp == p) coef++;
+        if (vp == best) coef--;
+        return (double)coef * (double)q;
+    }
+    return 0.0;
+}
+
+template <class W>
+__global__ void __launch_bounds__(256) k_afterburner_warp(ABArgs<W> a) {
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    const i64 hi_x = a.sc->split;
+    for (i64 x = gw; x < hi_x; x += nw) {
+        i32 i = a.cand[x];
+        i32 best = a.dest[i], p = a.part[i];
+        float multi = to_f(a.g.vtx_w[i]) * a.pm;
+        float igain = a.gain[i];
+        i32 hi = (i32)xorshift32((u32)i);
+        double ch = warp_canon_sum(a.g.rowptr[i], a.g.rowptr[i + 1],
+                                   [&](i64 j) { return ab_term(a, j, p, best, multi, igain, hi); });
+        if (lane_id() == 0) a.keep[x] = (igain + (float)ch) >= 0.0f ? 1 : 0;
+    }
+}
+
+template <class W>
+__global__ void __launch_bounds__(1024) k_afterburner_block(ABArgs<W> a) {
+    __shared__ double red[32];
+    const i64 lo = a.sc->split, hi_x = a.sc->num_cand;
+    for (i64 x = lo + blockIdx.x; x < hi_x; x += gridDim.x) {
+        i32 i = a.cand[x];
+        i32 best = a.dest[i], p = a.part[i];
+        float multi = to_f(a.g.vtx_w[i]) * a.pm;
+        float igain = a.gain[i];
+        i32 hi = (i32)xorshift32((u32)i);
+        double ch = block1024_canon_sum(a.g.rowptr[i], a.g.rowptr[i + 1],
+                                        [&](i64 j) { return ab_term(a, j, p, best, multi, igain, hi); }, red);
+        if (threadIdx.x == 0) a.keep[x] = (igain + (float)ch) >= 0.0f ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// compactions
+// ---------------------------------------------------------------------------
+struct CandFlag {
+    const i32* order1;
+    const i32* dest;
+    __device__ i64 operator()(i64 x) const { return dest[order1[x]] != NO_MOVE ? 1 : 0; }
+};
+struct CandEpi {
+    const i32* order1;
+    i32* cand;
+    i64 split_at;
+    i64* split;
+    __device__ void operator()(i64 x, i64 excl, i64 v) const {
+        if (v) cand[excl] = order1[x];
+        if (x == split_at) *split = excl;
+    }
+};
+struct KeepFlag {
+    const unsigned char* keep;
+    __device__ i64 operator()(i64 x) const { return keep[x]; }
+};
+struct ListEpi {
+    const i32* src;
+    i32* dst;
+    __device__ void operator()(i64 x, i64 excl, i64 v) const {
+        if (v) dst[excl] = src[x];
+    }
+};
+struct NewFlag {
+    const i32* moves;
+    const i32* dest;
+    __device__ i64 operator()(i64 x) const { return dest[moves[x]] == NEW_PART ? 1 : 0; }
+};
+struct UnusedFlag {
+    const unsigned char* has;
+    __device__ i64 operator()(i64 l) const { return has[l] ? 0 : 1; }
+};
+struct IdxEpi {
+    i32* dst;
+    __device__ void operator()(i64 x, i64 excl, i64 v) const {
+        if (v) dst[excl] = (i32)x;
+    }
+};
+
+template <class V>
+__global__ void k_set_split_if_end(LMScalars<V>* sc) {
+    sc->split = sc->num_cand;
+}
+
+// ---------------------------------------------------------------------------
+// set_new_cluster_ids (src/local_mover.cpp:217-274)
+// ---------------------------------------------------------------------------
+template <class V>
+__global__ void k_prep_new(LMScalars<V>* sc) {
+    sc->avail_k = sc->num_new > 0 ? sc->label_count : 0;
+}
+template <class V>
+__global__ void k_clear_has(unsigned char* has, const LMScalars<V>* sc) {
+    i64 L = sc->avail_k;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < L; i += (i64)gridDim.x * blockDim.x) has[i] = 0;
+}
+template <class V>
+__global__ void k_mark_has(unsigned char* has, const i32* part, i64 n, const LMScalars<V>* sc) {
+    if (sc->avail_k == 0) return;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) has[part[i]] = 1;
+}
+template <class V>
+__global__ void k_assign_new(const i32* newl, const i32* avail, i32* dest, const i32* part, i32* constraint, V* td,
+                             LMScalars<V>* sc, i64 capacity, int* err) {
+    i64 nn = sc->num_new, na = sc->num_avail, L = sc->label_count;
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nn; r += (i64)gridDim.x * blockDim.x) {
+        i32 x = newl[r];
+        i64 lab = r < na ? (i64)avail[r] : L + (r - na);
+        if (lab >= capacity) {
+            atomicExch(err, (int)DEV_ERR_LABEL);
+            continue;
+        }
+        dest[x] = (i32)lab;
+        if (constraint) constraint[lab] = constraint[part[x]];
+        if (r >= na) td[lab] = V(0);
+    }
+}
+template <class V>
+__global__ void k_finish_new(LMScalars<V>* sc, i64 capacity) {
+    if (sc->num_new > sc->num_avail) {
+        sc->label_count += sc->num_new - sc->num_avail;
+        if (sc->label_count > capacity) sc->label_count = capacity;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// perform_moves (src/local_mover.cpp:1241-1279)
+// ---------------------------------------------------------------------------
+template <class W>
+__global__ void k_apply_moves(DGraph<W> g, const i32* moves, i64 nm, const i32* dest, i32* part,
+                              typename Traits<W>::V* td, int* err) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < nm; x += (i64)gridDim.x * blockDim.x) {
+        i32 i = moves[x];
+        i32 b = dest[i], p = part[i];
+        if (b < 0) {  // an unresolved NEW_PART: never applied
+            atomicExch(err, (int)DEV_ERR_LABEL);
+            continue;
+        }
+        auto w = g.vtx_w[i];
+        vatomic_add(&td[p], -w);
+        vatomic_add(&td[b], w);
+        part[i] = b;
+    }
+}
+
+template <class W>
+__global__ void k_mark_affected(DGraph<W> g, const i32* moves, i64 nm, unsigned char* flags) {
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 x = gw; x < nm; x += nw) {
+        i32 i = moves[x];
+        if (lane_id() == 0) flags[i] = 1;
+        for (i64 j = g.rowptr[i] + lane_id(); j < g.rowptr[i + 1]; j += 32) flags[g.col[j]] = 1;
+    }
+}
+
+template <class V>
+struct SqIn;
+template <>
+struct SqIn<i64> {
+    const i64* td;
+    const i64* L;
+    __device__ i64 operator()(i64 i) const { return i < *L ? td[i] * td[i] : 0; }
+};
+template <>
+struct SqIn<double> {
+    const double* td;
+    const i64* L;
+    __device__ double operator()(i64 i) const { return i < *L ? td[i] * td[i] : 0.0; }
+};
+struct PvI64In {
+    const i64* a;
+    __device__ i64 operator()(i64 i) const { return a[i]; }
+};
+
+template <class V>
+__global__ void k_objective(LMScalars<V>* sc, double lambda) {
+    V cut_change = sc->pval_sum - sc->last_pval;
+    sc->last_pval = sc->pval_sum;
+    sc->uncut = sc->uncut + cut_change;
+    double m;
+    if constexpr (std::is_same<V, i64>::value) {
+        m = static_cast<double>(sc->uncut);
+        m = m - lambda * static_cast<double>(sc->sumsq_i);
+    } else {
+        m = sc->uncut;
+        m = m - lambda * sc->sumsq_d;
+    }
+    sc->obj = m;
+    sc->improved = m > sc->best_obj ? 1 : 0;
+    if (sc->improved) {
+        sc->best_obj = m;
+        sc->best_uncut = sc->uncut;
+        sc->best_label_count = sc->label_count;
+    }
+}
+
+template <class T, class V>
+__global__ void k_copy_if_improved(T* dst, const T* src, i64 n, const LMScalars<V>* sc, int use_label_count) {
+    if (!sc->improved) return;
+    i64 k = use_label_count ? sc->label_count : n;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < k; i += (i64)gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// afterburner_filter_strict (src/local_mover.cpp:131-213), O(k log k)
+// ---------------------------------------------------------------------------
+template <class W>
+__global__ void __launch_bounds__(256) k_strict_nb_warp(DGraph<W> g, const i32* moves, i64 lo, i64 hi,
+                                                        const i32* prio, const i32* dest, const i32* part,
+                                                        typename Traits<W>::V* nb) {
+    using V = typename Traits<W>::V;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 x = lo + gw; x < hi; x += nw) {
+        i32 i = moves[x];
+        i32 best = dest[i], p = part[i];
+        i32 pi = prio[i];
+        V r = VSum<V>::warp(g.rowptr[i], g.rowptr[i + 1], [&](i64 j) -> V {
+            i32 v = g.col[j];
+            if (!(prio[v] < pi)) return V(0);
+            int coef = 0;
+            i32 vp = dest[v];
+            if (vp == p) coef--;
+            if (vp == best && best != NEW_PART) coef++;
+            vp = part[v];
+            if (vp == p) coef++;
+            if (vp == best) coef--;
+            return V(coef) * V(g.wgt(j));
+        });
+        if (lane_id() == 0) nb[x] = r;
+    }
+}
+
+template <class W>
+__global__ void __launch_bounds__(1024) k_strict_nb_block(DGraph<W> g, const i32* moves, i64 lo, i64 hi,
+                                                          const i32* prio, const i32* dest, const i32* part,
+                                                          typename Traits<W>::V* nb) {
+    using V = typename Traits<W>::V;
+    __shared__ double red[32];
+    __shared__ unsigned long long acc;
+    for (i64 x = lo + blockIdx.x; x < hi; x += gridDim.x) {
+        i32 i = moves[x];
+        i32 best = dest[i], p = part[i];
+        i32 pi = prio[i];
+        auto term = [&](i64 j) -> V {
+            i32 v = g.col[j];
+            if (!(prio[v] < pi)) return V(0);
+            int coef = 0;
+            i32 vp = dest[v];
+            if (vp == p) coef--;
+            if (vp == best && best != NEW_PART) coef++;
+            vp = part[v];
+            if (vp == p) coef++;
+            if (vp == best) coef--;
+            return V(coef) * V(g.wgt(j));
+        };
+        V r;
+        if constexpr (std::is_same<V, double>::value) {
+            r = block1024_canon_sum(g.rowptr[i], g.rowptr[i + 1], term, red);
+        } else {
+            if (threadIdx.x == 0) acc = 0;
+            __syncthreads();
+            i64 s = 0;
+            for (i64 j = g.rowptr[i] + threadIdx.x; j < g.rowptr[i + 1]; j += 1024) s += term(j);
+            s = warp_sum_i64(s);
+            if (lane_id() == 0) ::atomicAdd(&acc, (unsigned long long)s);
+            __syncthreads();
+            r = (i64)acc;
+        }
+        if (threadIdx.x == 0) nb[x] = r;
+        __syncthreads();
+    }
+}
+
+__global__ void k_prio(const i32* moves, i64 k, i32* prio) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < k; x += (i64)gridDim.x * blockDim.x)
+        prio[moves[x]] = (i32)x;
+}
+
+template <class V>
+__global__ void k_strict_keys(const i32* moves, i64 k, const i32* dest, const i32* part, u64* kd, u64* kp, i32* id,
+                              i32* ip) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < k; x += (i64)gridDim.x * blockDim.x) {
+        i32 i = moves[x];
+        kd[x] = ((u64)(u32)dest[i] << 32) | (u64)x;
+        kp[x] = ((u64)(u32)part[i] << 32) | (u64)x;
+        id[x] = (i32)x;
+        ip[x] = (i32)x;
+    }
+}
+
+template <class V>
+__device__ __forceinline__ i64 lower_bound_u64(const u64* a, i64 k, u64 key) {
+    i64 lo = 0, hi = k;
+    while (lo < hi) {
+        i64 mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <class V>
+__device__ __forceinline__ V prefix_query(const u64* ks, const V* E, i64 k, i32 key, i64 x) {
+    u64 hk = (u64)(u32)key << 32;
+    i64 a = lower_bound_u64<V>(ks, k, hk | (u64)x);
+    i64 s = lower_bound_u64<V>(ks, k, hk);
+    return E[a] - E[s];
+}
+
+template <class W>
+__global__ void k_strict_oc(DGraph<W> g, const i32* moves, i64 k, const i32* dest, const i32* part, const float* gain,
+                            const typename Traits<W>::V* nb, const u64* ksd, const typename Traits<W>::V* Ed,
+                            const u64* ksp, const typename Traits<W>::V* Ep, float pm, double* oc) {
+    using V = typename Traits<W>::V;
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < k; x += (i64)gridDim.x * blockDim.x) {
+        i32 i = moves[x];
+        i32 best = dest[i], p = part[i];
+        float multi = to_f(g.vtx_w[i]) * pm;
+        V A = prefix_query<V>(ksd, Ed, k, p, x);
+        V B = best != NEW_PART ? prefix_query<V>(ksd, Ed, k, best, x) : V(0);
+        V C = prefix_query<V>(ksp, Ep, k, p, x);
+        V D = prefix_query<V>(ksp, Ep, k, best, x);
+        V S = ((C - A) + B) - D;
+        double t2 = -(double)multi * (double)S;
+        oc[x] = ((double)gain[i] + (double)nb[x]) + t2;
+    }
+}
+
+// first position of the maximum prefix value; writes num_moves = truncate
+template <class V>
+__global__ void __launch_bounds__(1024) k_strict_argmax(const double* pre, i64 k, LMScalars<V>* sc) {
+    __shared__ double bv[32];
+    __shared__ i64 bl[32];
+    double v = -INFINITY;
+    i64 loc = k;
+    for (i64 x = threadIdx.x; x < k; x += 1024)
+        if (pre[x] > v) {
+            v = pre[x];
+            loc = x;
+        }
+    for (int d = 16; d >= 1; d >>= 1) {
+        double ov = __shfl_xor_sync(FULL, v, d);
+        i64 ol = __shfl_xor_sync(FULL, loc, d);
+        if (ov > v || (ov == v && ol < loc)) {
+            v = ov;
+            loc = ol;
+        }
+    }
+    if (lane_id() == 0) {
+        bv[threadIdx.x >> 5] = v;
+        bl[threadIdx.x >> 5] = loc;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = bv[threadIdx.x];
+        loc = bl[threadIdx.x];
+        for (int d = 16; d >= 1; d >>= 1) {
+            double ov = __shfl_xor_sync(FULL, v, d);
+            i64 ol = __shfl_xor_sync(FULL, loc, d);
+            if (ov > v || (ov == v && ol < loc)) {
+                v = ov;
+                loc = ol;
+            }
+        }
+        if (threadIdx.x == 0) sc->num_moves = (loc < k && v > 0.0) ? loc + 1 : 0;
+    }
+}
+
+template <class V>
+__global__ void k_gather_vw(const i32* order, const i32* moves, const V* vw, i64 k, V* out) {
+    for (i64 y = blockIdx.x * (i64)blockDim.x + threadIdx.x; y < k; y += (i64)gridDim.x * blockDim.x)
+        out[y] = vw[moves[order[y]]];
+}
+struct I64ArrIn {
+    const i64* a;
+    i64 k;
+    __device__ i64 operator()(i64 i) const { return i < k ? a[i] : 0; }
+};
+struct I64ExclOut {
+    i64* E;
+    __device__ void operator()(i64 i, i64 excl, i64) const { E[i] = excl; }
+};
+
+// ---------------------------------------------------------------------------
+// relabel_contiguously (src/local_mover.cpp:100-129)
+// ---------------------------------------------------------------------------
+__global__ void k_mark_used(unsigned char* used, const i32* lab, i64 n) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) used[lab[i]] = 1;
+}
+struct UsedFlag {
+    const unsigned char* used;
+    __device__ i64 operator()(i64 l) const { return used[l] ? 1 : 0; }
+};
+template <class V>
+struct RelabelEpi {
+    i32* newid;
+    const V* td;
+    V* td_out;
+    __device__ void operator()(i64 l, i64 excl, i64 v) const {
+        if (v) {
+            newid[l] = (i32)excl;
+            td_out[excl] = td[l];
+        }
+    }
+};
+__global__ void k_remap(i32* lab, i64 n, const i32* newid) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        lab[i] = newid[lab[i]];
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+inline int grid_for(Context& ctx, i64 work, int per_block, int max_per_sm = 16) {
+    return (int)std::max<i64>(1, std::min<i64>(ceil_div(std::max<i64>(work, 1), per_block), (i64)ctx.num_sms * max_per_sm));
+}
+
+template <class W>
+struct Mover {
+    using V = typename Traits<W>::V;
+    Context& ctx;
+    const Graph<W>& g;
+    const Ordering& ord;
+    i64 n;
+    i64 cap;  // label capacity
+    DBuf<i32> part, dest, cand, moves, newl, avail, prio, tmp_i32;
+    DBuf<float> gain;
+    DBuf<V> pvals, pvals_clone, td_curr;
+    DBuf<unsigned char> flags, keep, has;
+    DBuf<LMScalars<V>> sc;
+    DBuf<i32> gkeys;
+    DBuf<V> gvals;
+    i64 gcap = 0;
+    bool cdata_init = false;
+
+    Mover(Context& c, const Graph<W>& gr, const Ordering& o, i64 capacity)
+        : ctx(c), g(gr), ord(o), n(gr.n), cap(capacity) {
+        i64 nn = std::max<i64>(n, 1);
+        part = DBuf<i32>(ctx, nn);
+        dest = DBuf<i32>(ctx, nn);
+        cand = DBuf<i32>(ctx, nn);
+        moves = DBuf<i32>(ctx, nn);
+        newl = DBuf<i32>(ctx, nn);
+        avail = DBuf<i32>(ctx, std::max<i64>(cap, 1));
+        gain = DBuf<float>(ctx, nn);
+        pvals = DBuf<V>(ctx, nn);
+        pvals_clone = DBuf<V>(ctx, nn);
+        td_curr = DBuf<V>(ctx, std::max<i64>(cap, 1));
+        flags = DBuf<unsigned char>(ctx, nn);
+        keep = DBuf<unsigned char>(ctx, nn);
+        has = DBuf<unsigned char>(ctx, std::max<i64>(cap, 1));
+        sc = DBuf<LMScalars<V>>(ctx, 1);
+        PGGC_CUDA(cudaMemsetAsync(flags.p, 0, nn, ctx.stream));
+        if (ord.n_huge > 0) {
+            gcap = next_pow2_u32((u32)std::min<i64>(2 * ord.max_deg, (i64)1 << 30));
+            i64 nb = std::min<i64>(ord.n_huge, 32);
+            gkeys = DBuf<i32>(ctx, gcap * nb);
+            gvals = DBuf<V>(ctx, gcap * nb);
+        }
+    }
+
+    SelArgs<W> sel_args(float fr, bool initial, const i32* constraint, const V* td, const i32* partp,
+                        const V* pv, i32* destp, float* gainp, const i64* lcount, float pm) {
+        SelArgs<W> a;
+        a.g = g.view();
+        a.part = partp;
+        a.dest = destp;
+        a.gain = gainp;
+        a.pvals = pv;
+        a.td = td;
+        a.constraint = constraint;
+        a.label_count = lcount;
+        a.pm = pm;
+        a.fr = fr;
+        a.initial = initial ? 1 : 0;
+        a.err = ctx.d_err;
+        return a;
+    }
+
+    template <bool CON>
+    void launch_select_t(const SelArgs<W>& a) {
+        if (ord.off_large > 0) {
+            int grid = grid_for(ctx, ceil_div(ord.off_large, SELW_WARPS), 1, 16);
+            k_select_warp<W, CON><<<grid, SELW_WARPS * 32, 0, ctx.stream>>>(a, ord.order1.p, ord.off_large);
+            PGGC_LAUNCH_CHECK();
+        }
+        i64 nb = n - ord.off_large;
+        if (nb > 0) {
+            size_t sm = (sizeof(V) + sizeof(i32)) * SEL_TS_MAX;
+            PGGC_CUDA(cudaFuncSetAttribute(k_select_block<W, CON, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm));
+            int grid = (int)std::min<i64>(nb, (i64)ctx.num_sms * 2);
+            k_select_block<W, CON, false><<<grid, 256, sm, ctx.stream>>>(a, ord.order1.p + ord.off_large, nb, nullptr,
+                                                                         nullptr, 0);
+            PGGC_LAUNCH_CHECK();
+        }
+        if (ord.n_huge > 0) {
+            int grid = (int)std::min<i64>(ord.n_huge, 32);
+            k_select_block<W, CON, true><<<grid, 256, 0, ctx.stream>>>(a, ord.huge.p, ord.n_huge, gkeys.p, gvals.p, gcap);
+            PGGC_LAUNCH_CHECK();
+        }
+    }
+    void launch_select(const SelArgs<W>& a, bool constrained) {
+        if (constrained) launch_select_t<true>(a);
+        else launch_select_t<false>(a);
+    }
+
+    // candidates (order1 order) -> cand, sc.num_cand, sc.split
+    void compact_candidates() {
+        LMScalars<V>* s = sc.p;
+        scan_apply(ctx, CandFlag{ord.order1.p, dest.p},
+                   CandEpi{ord.order1.p, cand.p, ord.off_large2 < n ? ord.off_large2 : -1, &s->split}, n, nullptr,
+                   &s->num_cand);
+        if (ord.off_large2 >= n) {
+            k_set_split_if_end<V><<<1, 1, 0, ctx.stream>>>(s);
+            PGGC_LAUNCH_CHECK();
+        }
+    }
+
+    void afterburner(float pm) {
+        ABArgs<W> a;
+        a.g = g.view();
+        a.part = part.p;
+        a.dest = dest.p;
+        a.gain = gain.p;
+        a.pm = pm;
+        a.cand = cand.p;
+        a.keep = keep.p;
+        a.sc = sc.p;
+        int grid = grid_for(ctx, ceil_div(n, 8), 1, 16);
+        k_afterburner_warp<W><<<grid, 256, 0, ctx.stream>>>(a);
+        PGGC_LAUNCH_CHECK();
+        i64 nm = n - ord.off_large2;
+        if (nm > 0) {
+            k_afterburner_block<W><<<(int)std::min<i64>(nm, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(a);
+            PGGC_LAUNCH_CHECK();
+        }
+        scan_apply(ctx, KeepFlag{keep.p}, ListEpi{cand.p, moves.p}, n, &sc.p->num_cand, &sc.p->num_moves);
+    }
+
+    void set_new_cluster_ids(i64 nmoves_host, i32* constraint) {
+        LMScalars<V>* s = sc.p;
+        scan_apply(ctx, NewFlag{moves.p, dest.p}, ListEpi{moves.p, newl.p}, nmoves_host, nullptr, &s->num_new);
+        k_prep_new<V><<<1, 1, 0, ctx.stream>>>(s);
+        PGGC_LAUNCH_CHECK();
+        k_clear_has<V><<<grid_for(ctx, cap, 256), 256, 0, ctx.stream>>>(has.p, s);
+        PGGC_LAUNCH_CHECK();
+        k_mark_has<V><<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(has.p, part.p, n, s);
+        PGGC_LAUNCH_CHECK();
+        scan_apply(ctx, UnusedFlag{has.p}, IdxEpi{avail.p}, cap, &s->avail_k, &s->num_avail);
+        k_assign_new<V><<<grid_for(ctx, nmoves_host, 256), 256, 0, ctx.stream>>>(
+            newl.p, avail.p, dest.p, part.p, constraint, td_curr.p, s, cap, ctx.d_err);
+        PGGC_LAUNCH_CHECK();
+        k_finish_new<V><<<1, 1, 0, ctx.stream>>>(s, cap);
+        PGGC_LAUNCH_CHECK();
+    }
+
+    void perform_moves(i64 nm, double lambda, i64 label_bound) {
+        auto gv = g.view();
+        k_apply_moves<W><<<grid_for(ctx, nm, 256), 256, 0, ctx.stream>>>(gv, moves.p, nm, dest.p, part.p, td_curr.p,
+                                                                        ctx.d_err);
+        PGGC_LAUNCH_CHECK();
+        if (!cdata_init) {
+            cdata_init = true;
+            own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 0, nullptr, nullptr);
+            fill<i32>(ctx, dest.p, n, NULL_PART);
+        } else {
+            k_mark_affected<W><<<grid_for(ctx, ceil_div(nm, 8), 1, 16), 256, 0, ctx.stream>>>(gv, moves.p, nm, flags.p);
+            PGGC_LAUNCH_CHECK();
+            own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 1, flags.p, dest.p);
+        }
+        update_objective_dev(lambda, label_bound);
+    }
+
+    void update_objective_dev(double lambda, i64 label_bound) {
+        LMScalars<V>* s = sc.p;
+        if constexpr (std::is_same<V, i64>::value) {
+            sum_i64(ctx, PvI64In{pvals.p}, n, &s->pval_sum);
+            sum_i64(ctx, SqIn<i64>{td_curr.p, &s->label_count}, label_bound, &s->sumsq_i);
+        } else {
+            det_reduce(ctx, DArrIn{pvals.p}, n, &s->pval_sum);
+            det_reduce(ctx, SqIn<double>{td_curr.p, &s->label_count}, label_bound, &s->sumsq_d);
+        }
+        k_objective<V><<<1, 1, 0, ctx.stream>>>(s, lambda);
+        PGGC_LAUNCH_CHECK();
+    }
+
+    void copy_if_improved(i32* best_part, V* td_best, i64 label_bound) {
+        LMScalars<V>* s = sc.p;
+        k_copy_if_improved<i32, V><<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(best_part, part.p, n, s, 0);
+        PGGC_LAUNCH_CHECK();
+        k_copy_if_improved<V, V><<<grid_for(ctx, label_bound, 256), 256, 0, ctx.stream>>>(td_best, td_curr.p,
+                                                                                           label_bound, s, 1);
+        PGGC_LAUNCH_CHECK();
+        k_copy_if_improved<V, V><<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(pvals_clone.p, pvals.p, n, s, 0);
+        PGGC_LAUNCH_CHECK();
+    }
+
+    // strict prefix selection over moves[0..k); writes sc.num_moves
+    void strict_filter(i64 k, i64 split_host, float pm) {
+        auto gv = g.view();
+        prio.ensure(ctx, std::max<i64>(n, 1));
+        fill<i32>(ctx, prio.p, n, (i32)std::min<i64>(n + 1, 2147483647));
+        k_prio<<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(moves.p, k, prio.p);
+        PGGC_LAUNCH_CHECK();
+        DBuf<V> nb(ctx, k);
+        if (split_host > 0) {
+            k_strict_nb_warp<W><<<grid_for(ctx, ceil_div(split_host, 8), 1, 16), 256, 0, ctx.stream>>>(
+                gv, moves.p, 0, split_host, prio.p, dest.p, part.p, nb.p);
+            PGGC_LAUNCH_CHECK();
+        }
+        if (k > split_host) {
+            k_strict_nb_block<W><<<(int)std::min<i64>(k - split_host, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(
+                gv, moves.p, split_host, k, prio.p, dest.p, part.p, nb.p);
+            PGGC_LAUNCH_CHECK();
+        }
+        DBuf<u64> kd(ctx, k), kp(ctx, k), kt(ctx, k);
+        DBuf<i32> od(ctx, k), op(ctx, k), ot(ctx, k);
+        k_strict_keys<V><<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(moves.p, k, dest.p, part.p, kd.p, kp.p, od.p,
+                                                                        op.p);
+        PGGC_LAUNCH_CHECK();
+        radix_sort_pairs<i32>(ctx, kd.p, od.p, k, 32, 64, kt.p, ot.p);
+        radix_sort_pairs<i32>(ctx, kp.p, op.p, k, 32, 64, kt.p, ot.p);
+        DBuf<V> wd(ctx, k), wp(ctx, k), Ed(ctx, k + 1), Ep(ctx, k + 1);
+        k_gather_vw<V><<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(od.p, moves.p, g.vtx_w.p, k, wd.p);
+        k_gather_vw<V><<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(op.p, moves.p, g.vtx_w.p, k, wp.p);
+        PGGC_LAUNCH_CHECK();
+        if constexpr (std::is_same<V, i64>::value) {
+            scan_apply(ctx, I64ArrIn{wd.p, k}, I64ExclOut{Ed.p}, k + 1, nullptr, nullptr);
+            scan_apply(ctx, I64ArrIn{wp.p, k}, I64ExclOut{Ep.p}, k + 1, nullptr, nullptr);
+        } else {
+            // exclusive prefix = shifted canonical inclusive scan
+            PGGC_CUDA(cudaMemsetAsync(Ed.p, 0, sizeof(double), ctx.stream));
+            PGGC_CUDA(cudaMemsetAsync(Ep.p, 0, sizeof(double), ctx.stream));
+            det_scan(ctx, DArrIn{wd.p}, Ed.p + 1, k);
+            det_scan(ctx, DArrIn{wp.p}, Ep.p + 1, k);
+        }
+        DBuf<double> oc(ctx, k), pre(ctx, k);
+        k_strict_oc<W><<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(gv, moves.p, k, dest.p, part.p, gain.p, nb.p, kd.p,
+                                                                       Ed.p, kp.p, Ep.p, pm, oc.p);
+        PGGC_LAUNCH_CHECK();
+        det_scan(ctx, DArrIn{oc.p}, pre.p, k);
+        k_strict_argmax<V><<<1, 1024, 0, ctx.stream>>>(pre.p, k, sc.p);
+        PGGC_LAUNCH_CHECK();
+    }
+
+    void relabel(i32* best_part, ClusterState<V>& best) {
+        i64 L = best.label_count;
+        DBuf<unsigned char> used(ctx, std::max<i64>(L, 1));
+        DBuf<i32> newid(ctx, std::max<i64>(L, 1));
+        DBuf<V> td2(ctx, std::max<i64>(L, 1));
+        DBuf<i64> tot(ctx, 1);
+        PGGC_CUDA(cudaMemsetAsync(used.p, 0, std::max<i64>(L, 1), ctx.stream));
+        k_mark_used<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(used.p, best_part, n);
+        PGGC_LAUNCH_CHECK();
+        scan_apply(ctx, UsedFlag{used.p}, RelabelEpi<V>{newid.p, best.total_deg.p, td2.p}, L, nullptr, tot.p);
+        k_remap<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(best_part, n, newid.p);
+        PGGC_LAUNCH_CHECK();
+        i64 t = ctx.read1(tot.p);
+        copy_d2d(ctx, best.total_deg.p, td2.p, t);
+        best.label_count = t;
+    }
+};
+
+template <class W>
+void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_part,
+                ClusterState<typename Traits<W>::V>& best, bool is_initial, bool constrained, i32* constraint,
+                bool enable_sa, bool strict, int sweep_limit, MoveStats* stats) {
+    using V = typename Traits<W>::V;
+    const i64 n = g.n;
+    if (n == 0) return;
+    if (best.capacity < best.label_count) throw InvalidArg("cluster state capacity below label count");
+    Mover<W> m(ctx, g, ord, best.capacity);
+    const float pm = (float)best.lambda;
+    // curr_state.copy(best_state); part = best_part (src/local_mover.cpp:1365-1368)
+    LMScalars<V> h{};
+    h.label_count = best.label_count;
+    h.best_label_count = best.label_count;
+    h.uncut = best.uncut;
+    h.best_uncut = best.uncut;
+    h.obj = best.obj;
+    h.best_obj = best.obj;
+    copy_d2d(ctx, m.part.p, best_part, n);
+    copy_d2d(ctx, m.td_curr.p, best.total_deg.p, best.label_count);
+    fill<i32>(ctx, m.dest.p, n, NULL_PART);
+    if (!is_initial) {
+        m.cdata_init = true;
+        own_weights_impl<W>(ctx, g, ord, m.part.p, m.pvals.p, 0, nullptr, nullptr);
+    } else {
+        m.cdata_init = false;
+        PGGC_CUDA(cudaMemsetAsync(m.pvals.p, 0, sizeof(V) * n, ctx.stream));
+    }
+    PGGC_CUDA(cudaMemcpyAsync(m.sc.p, &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream));
+    if (!is_initial) {
+        if constexpr (std::is_same<V, i64>::value) sum_i64(ctx, PvI64In{m.pvals.p}, n, &m.sc.p->last_pval);
+        else det_reduce(ctx, DArrIn{m.pvals.p}, n, &m.sc.p->last_pval);
+    }
+    copy_d2d(ctx, m.pvals_clone.p, m.pvals.p, n);
+
+    i64 label_bound = best.label_count;  // host upper bound of sc.label_count
+    int sweeps = 0;
+    i64 total_moves = 0;
+    auto budget = [&]() { return sweep_limit < 0 || sweeps < sweep_limit; };
+
+    if (!strict) {
+        const float ratios[2] = {0.75f, 0.25f};
+        const int limits[2] = {4, 2};
+        int iter_count = 0;
+        for (int x = 0; x < 2; x++) {
+            float fr = enable_sa ? ratios[x] : 0.0f;
+            int count = 0;
+            while (count++ < limits[x]) {
+                if (!budget()) break;
+                sweeps++;
+                iter_count++;
+                auto a = m.sel_args(fr, !m.cdata_init, constraint, m.td_curr.p, m.part.p, m.pvals.p, m.dest.p,
+                                    m.gain.p, &m.sc.p->label_count, pm);
+                m.launch_select(a, constrained);
+                m.compact_candidates();
+                m.afterburner(pm);
+                const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
+                i64 ncand = hs->num_cand, nm = hs->num_moves;
+                if (ncand == 0 || nm == 0) break;
+                if (iter_count > 1 || !is_initial) m.set_new_cluster_ids(nm, constrained ? constraint : nullptr);
+                label_bound = std::min<i64>(label_bound + nm, m.cap);
+                m.perform_moves(nm, best.lambda, label_bound);
+                m.copy_if_improved(best_part, best.total_deg.p, label_bound);
+                total_moves += nm;
+            }
+        }
+    } else {
+        for (int it = 0; it < 6; it++) {
+            if (!budget()) break;
+            sweeps++;
+            auto a = m.sel_args(0.0f, !m.cdata_init, constraint, m.td_curr.p, m.part.p, m.pvals.p, m.dest.p, m.gain.p,
+                                &m.sc.p->label_count, pm);
+            m.launch_select(a, constrained);
+            m.compact_candidates();
+            const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
+            i64 k = hs->num_cand, split = hs->split;
+            if (k == 0) break;
+            copy_d2d(ctx, m.moves.p, m.cand.p, k);
+            PGGC_CUDA(cudaMemcpyAsync(&m.sc.p->num_moves, &m.sc.p->num_cand, sizeof(i64), cudaMemcpyDeviceToDevice,
+                                      ctx.stream));
+            if (it > 0 || !is_initial) m.set_new_cluster_ids(k, constrained ? constraint : nullptr);
+            label_bound = std::min<i64>(label_bound + k, m.cap);
+            m.strict_filter(k, split, pm);
+            i64 nm = ctx.read1(&m.sc.p->num_moves);
+            if (nm == 0) break;
+            m.perform_moves(nm, best.lambda, label_bound);
+            m.copy_if_improved(best_part, best.total_deg.p, label_bound);
+            fill<i32>(ctx, m.dest.p, n, NULL_PART);
+            total_moves += nm;
+        }
+    }
+    const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
+    best.label_count = hs->best_label_count;
+    best.uncut = hs->best_uncut;
+    best.obj = hs->best_obj;
+    ctx.check_device_error();
+    m.relabel(best_part, best);
+    if (stats) {
+        stats->sweeps += sweeps;
+        stats->moves += total_moves;
+    }
+}
+
+template <class W>
+i64 select_pass(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* part,
+                const typename Traits<W>::V* pvals, ClusterState<typename Traits<W>::V>& cs, i32* dest, float* gain,
+                float filter_ratio, bool initial, bool constrained, const i32* constraint) {
+    using V = typename Traits<W>::V;
+    Mover<W> m(ctx, g, ord, cs.capacity);
+    LMScalars<V> h{};
+    h.label_count = cs.label_count;
+    PGGC_CUDA(cudaMemcpyAsync(m.sc.p, &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream));
+    auto a = m.sel_args(filter_ratio, initial, constraint, cs.total_deg.p, part, pvals, dest, gain,
+                        &m.sc.p->label_count, (float)cs.lambda);
+    m.launch_select(a, constrained);
+    scan_apply(ctx, CandFlag{ord.order1.p, dest}, CandEpi{ord.order1.p, m.cand.p, -1, nullptr}, g.n, nullptr,
+               &m.sc.p->num_cand);
+    i64 k = ctx.read1(&m.sc.p->num_cand);
+    ctx.check_device_error();
+    return k;
+}
+
+#define PGGC_INST_LM(W)                                                                                             \
+    template void local_move<W>(Context&, const Graph<W>&, const Ordering&, i32*, ClusterState<Traits<W>::V>&, bool, \
+                                bool, i32*, bool, bool, int, MoveStats*);                                           \
+    template i64 select_pass<W>(Context&, const Graph<W>&, const Ordering&, const i32*, const Traits<W>::V*,         \
+                                ClusterState<Traits<W>::V>&, i32*, float*, float, bool, bool, const i32*);          \
+    template void own_weights<W>(Context&, const Graph<W>&, const Ordering&, const i32*, Traits<W>::V*);
+PGGC_INST_LM(i32)
+PGGC_INST_LM(float)
+
+}  // namespace pggc

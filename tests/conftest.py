@@ -1,0 +1,20 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the sm_100a kernels")
+    config.addinivalue_line("markers", "slow: larger workloads")
+
+
+@pytest.fixture(scope="session")
+def mem():
+    from pennsylvaniagpugraphclustering_b200 import memory_store
+    m = memory_store(0)
+    yield m

@@ -1,0 +1,245 @@
+"""GPU parity: every hot-path function through the C ABI against the CPU oracle.
+
+Integer and FP32-weighted graphs are compared bit-exactly: both sides use the
+same canonical arithmetic (FP32 gain expressions operation by operation, int64
+or FP64 sums in a fixed association, smallest-id tie breaks, sorted coarse rows,
+MurmurHash3 random picks), so any difference is a bug.
+"""
+import numpy as np
+import pytest
+
+import pennsylvaniagpugraphclustering_b200 as pg
+from oracle import oracle as O
+
+from . import graphs as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(mem, hg, objective):
+    uniform = objective in (pg.OBJ_MOD, pg.OBJ_CPM) or hg.w is None
+    w = None if uniform else hg.w
+    og = O.Graph(hg.rowptr, hg.col, w, objective=objective)
+    wg = pg.weighted_graph(mem, hg.rowptr, hg.col, w, objective=objective)
+    return og, wg
+
+
+CASES = [
+    ("two_cliques", G.two_cliques, pg.OBJ_MOD),
+    ("ring_of_cliques", G.ring_of_cliques, pg.OBJ_MOD),
+    ("star", G.star, pg.OBJ_MOD),
+    ("path", G.path, pg.OBJ_MOD),
+    ("isolated", G.with_isolated, pg.OBJ_MOD),
+    ("sbm", G.small_sbm, pg.OBJ_MOD),
+    ("rmat12", G.small_rmat, pg.OBJ_MOD),
+    ("dcsbm_wmod", G.small_dcsbm, pg.OBJ_WMOD),
+    ("dcsbm_mod", G.small_dcsbm, pg.OBJ_MOD),
+    ("hub_wmod", G.hub_graph, pg.OBJ_WMOD),
+    ("hub_mod", G.hub_graph, pg.OBJ_MOD),
+]
+IDS = [c[0] for c in CASES]
+
+_CACHE = {}
+
+
+def case_graph(name):
+    if name not in _CACHE:
+        for nm, fn, obj in CASES:
+            if nm == name:
+                _CACHE[name] = (fn(), obj)
+    return _CACHE[name]
+
+
+@pytest.mark.parametrize("name", IDS)
+def test_vertex_weights_and_objective(mem, name):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    _, _, _, vw_o = og.arrays()
+    _, _, _, vw_g = wg.to_host()
+    assert np.array_equal(vw_o, vw_g)
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    io = cd_o.info()
+    assert io["lambda"] == cd_g.lambda_
+    assert io["obj"] == cd_g.obj
+    assert io["label_count"] == cd_g.label_count
+
+
+@pytest.mark.parametrize("name", IDS)
+def test_generate_orderings(mem, name):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    o1, o2, off = O.generate_orderings(hg.rowptr)
+    g1, g2, goff = pg.generate_orderings(mem, wg)
+    assert np.array_equal(o1, g1)
+    assert np.array_equal(o2, g2)
+    assert np.array_equal(off, goff)
+
+
+def _random_map(n, nc, seed):
+    rng = np.random.default_rng(seed)
+    m = rng.integers(0, nc, n).astype(np.int32)
+    m[:nc] = np.arange(nc, dtype=np.int32)  # every coarse id used
+    return m
+
+
+@pytest.mark.parametrize("name", IDS)
+@pytest.mark.parametrize("ratio", [2, 7])
+def test_build_coarse_graph(mem, name, ratio):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    nc = max(1, hg.n // ratio)
+    vcmap = _random_map(hg.n, nc, ratio)
+    co = O.build_coarse_graph(og, vcmap, nc)
+    cg = pg.build_coarse_graph(mem, wg, vcmap, nc)
+    ro, col_o, w_o, vw_o = co.arrays()
+    rg, col_g, w_g, vw_g = cg.to_host()
+    assert np.array_equal(ro, rg)
+    assert np.array_equal(col_o, col_g)
+    assert np.array_equal(w_o, w_g)
+    assert np.array_equal(vw_o, vw_g)
+    # rows sorted, no self loops
+    for c in range(min(nc, 200)):
+        row = col_g[rg[c]:rg[c + 1]]
+        assert np.all(np.diff(row) > 0)
+        assert not np.any(row == c)
+
+
+@pytest.mark.parametrize("name", IDS)
+@pytest.mark.parametrize("fr", [0.0, 0.25, 0.75])
+@pytest.mark.parametrize("initial", [True, False])
+def test_select_pass(mem, name, fr, initial):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    n = hg.n
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    if initial:
+        part = np.arange(n, dtype=np.int32)
+        pv = np.zeros(n, wg.vdtype)
+    else:
+        # a coarse random partition with its exact state
+        L = max(1, n // 5)
+        part = _random_map(n, L, 11)
+        _, _, w, vw = og.arrays()
+        td = np.zeros(L, wg.vdtype)
+        np.add.at(td, part, vw)
+        src = np.repeat(np.arange(n), np.diff(hg.rowptr))
+        same = part[src] == part[hg.col]
+        ww = np.ones(hg.nnz) if w is None else w.astype(np.float64)
+        pv = np.zeros(n, np.float64)
+        np.add.at(pv, src[same], ww[same])
+        pv = pv.astype(wg.vdtype)
+        uncut = pv.sum()
+        cd_o.set_state(td, uncut)
+        cd_g.set_state(L, td, uncut)
+    dest0 = np.full(n, pg.NULL_PART, np.int32)
+    dest0[::7] = pg.NO_MOVE
+    do, go, ko = O.select(og, cd_o, part, pv, dest0, fr, initial)
+    dg, gg_, kg = pg.select_pass(mem, wg, cd_g, part, pv, dest0, fr, initial)
+    assert ko == kg
+    assert np.array_equal(do, dg)
+    assert np.array_equal(go.view(np.int32), gg_.view(np.int32))
+
+
+@pytest.mark.parametrize("name", IDS)
+@pytest.mark.parametrize("limit", [1, 2, -1])
+def test_local_move_initial(mem, name, limit):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    n = hg.n
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    part = np.arange(n, dtype=np.int32)
+    po, st, _ = O.local_move(og, cd_o, part, True, enable_sa=True, sweep_limit=limit)
+    pgp = part.copy()
+    pg.local_move(mem, wg, pgp, cd_g, True, sweep_limit=limit)
+    assert np.array_equal(po, pgp)
+    io = cd_o.info()
+    assert io["label_count"] == cd_g.label_count
+    assert io["obj"] == cd_g.obj
+    assert np.array_equal(cd_o.total_deg(), cd_g.total_deg())
+
+
+@pytest.mark.parametrize("name", IDS)
+@pytest.mark.parametrize("strict", [False, True])
+def test_local_move_from_partition(mem, name, strict):
+    """Non-initial call (conn tables built from an existing partition), SA off / strict."""
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    n = hg.n
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    part = np.arange(n, dtype=np.int32)
+    po, _, _ = O.local_move(og, cd_o, part, True, sweep_limit=2)
+    pgp = part.copy()
+    pg.local_move(mem, wg, pgp, cd_g, True, sweep_limit=2)
+    assert np.array_equal(po, pgp)
+    po2, _, _ = O.local_move(og, cd_o, po, False, enable_sa=False, strict=strict)
+    pg2 = pgp.copy()
+    if strict:
+        pg.local_move_strict(mem, wg, pg2, cd_g, False)
+    else:
+        pg.local_move(mem, wg, pg2, cd_g, False, enable_simulated_annealing=False)
+    assert np.array_equal(po2, pg2)
+    assert cd_o.info()["obj"] == cd_g.obj
+    assert cd_o.info()["label_count"] == cd_g.label_count
+
+
+@pytest.mark.parametrize("name", IDS)
+def test_coarsen_leidenR(mem, name):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    n = hg.n
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    part = np.arange(n, dtype=np.int32)
+    po, _, _ = O.local_move(og, cd_o, part, True)
+    pgp = part.copy()
+    pg.local_move(mem, wg, pgp, cd_g, True)
+    assert np.array_equal(po, pgp)
+    for seeds in [(1, 2), (12345, 678), (0xDEADBEEF, 0x12345678)]:
+        vo, nco = O.coarsen_leidenR(og, cd_o, po, *seeds)
+        vg, ncg = pg.coarsen_leidenR(mem, wg, pgp, cd_g, *seeds)
+        assert nco == ncg
+        assert np.array_equal(vo, vg)
+
+
+@pytest.mark.parametrize("name", IDS)
+@pytest.mark.parametrize("method", [pg.METHOD_LOUVAIN, pg.METHOD_LEIDEN, pg.METHOD_LEIDEN_PLUS])
+def test_run_clustering(mem, name, method):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    lo, so = O.run_clustering(og, cd_o, method=method, ex_iters=0, seed=7)
+    lg, sg = pg.run_clustering(mem, wg, cd_g, method=method, ex_iters=0, seed=7)
+    assert np.array_equal(lo, lg)
+    assert so.objective == sg["objective"]
+    assert so.label_count == sg["label_count"]
+    assert so.levels == sg["levels"]
+    if method == pg.METHOD_LEIDEN:
+        # every pLeiden cluster is connected
+        assert O.connected_components(hg.rowptr, hg.col, lg) == len(np.unique(lg))
+
+
+@pytest.mark.parametrize("name", ["sbm", "dcsbm_wmod", "rmat12"])
+def test_run_clustering_ex_iters(mem, name):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    lo, so = O.run_clustering(og, cd_o, method=pg.METHOD_LEIDEN_PLUS, ex_iters=-1, seed=3)
+    lg, sg = pg.run_clustering(mem, wg, cd_g, method=pg.METHOD_LEIDEN_PLUS, ex_iters=-1, seed=3)
+    assert np.array_equal(lo, lg)
+    assert so.objective == sg["objective"]
+
+
+@pytest.mark.parametrize("name", IDS)
+def test_verify_objective(mem, name):
+    hg, obj = case_graph(name)
+    og, wg = _pair(mem, hg, obj)
+    labels = _random_map(hg.n, max(1, hg.n // 9), 5)
+    vo, ro = O.verify_objective(og, labels, obj)
+    vg, rg = pg.verify_objective(mem, wg, labels, obj)
+    assert vo == vg and ro == rg
