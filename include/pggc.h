@@ -64,6 +64,18 @@ const char* pggc_last_error(void);
 /* build-time identification, e.g. "pggc-b200 sm_100a" */
 const char* pggc_version(void);
 
+/* kernels launched by this library in this process so far */
+uint64_t pggc_launch_count(void);
+
+/* Per-kernel-family timing (CUDA events on the context stream) and algorithmic
+ * byte counts, for roofline reporting; the counterpart of the reference's
+ * EXTRA_TIMING measurements (src/clustering_methods.cpp:78-108).  Families:
+ * "select_warp", "select_block", "select_huge", "afterburner_warp",
+ * "afterburner_block", "own_weights", "contract", "leiden_refine", "orderings". */
+pggc_status pggc_profile_enable(pggc_context* ctx, int on);
+pggc_status pggc_profile_reset(pggc_context* ctx);
+pggc_status pggc_profile_read(pggc_context* ctx, const char* family, int64_t* launches, double* ms, double* bytes);
+
 /* ---- memory_store (interface/memory_store.hpp:84-90) ---------------------- */
 pggc_status pggc_context_create(int device, pggc_context** out);
 pggc_status pggc_context_destroy(pggc_context* ctx);

@@ -44,6 +44,7 @@
 #include <limits>
 #include <memory>
 #include <numeric>
+#include <stdexcept>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1094,6 +1095,7 @@ struct Engine {
         SplitMix64 rng(seed);
         while (true) {
             const G& c = *levels.back();
+            if ((i64)levels.size() > 4096) throw std::runtime_error("multilevel hierarchy exceeded 4096 levels");
             double old_obj = rfd.obj;
             bool init = !improve && levels.size() == 1;
             ord = generate_orderings(c.rowptr.data(), c.n);
@@ -1157,6 +1159,7 @@ struct Engine {
         bool drop = constrained;
         while (true) {
             const G& c = *levels.back();
+            if ((i64)levels.size() > 4096) throw std::runtime_error("multilevel hierarchy exceeded 4096 levels");
             std::vector<i32> part(c.n);
             for (i64 x = 0; x < c.n; x++) part[x] = (i32)x;
             ord = generate_orderings(c.rowptr.data(), c.n);

@@ -49,6 +49,11 @@ _PP = ctypes.POINTER(ctypes.c_void_p)
 _SIGS = {
     "pggc_last_error": (ctypes.c_char_p, []),
     "pggc_version": (ctypes.c_char_p, []),
+    "pggc_launch_count": (_u64, []),
+    "pggc_profile_enable": (_ci, [_vp, _ci]),
+    "pggc_profile_reset": (_ci, [_vp]),
+    "pggc_profile_read": (_ci, [_vp, ctypes.c_char_p, ctypes.POINTER(_i64), ctypes.POINTER(_dbl),
+                               ctypes.POINTER(_dbl)]),
     "pggc_context_create": (_ci, [_ci, _PP]),
     "pggc_context_destroy": (_ci, [_vp]),
     "pggc_context_stream": (_ci, [_vp, _PP]),

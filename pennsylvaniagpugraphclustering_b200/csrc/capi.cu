@@ -6,6 +6,10 @@
 
 using namespace pggc;
 
+namespace pggc {
+std::atomic<unsigned long long> g_kernel_launches{0};
+}
+
 struct pggc_context {
     std::unique_ptr<Context> ctx;
 };
@@ -113,6 +117,41 @@ void check_labels(Context& c, const i32* labels, i64 n, i64 hi, const char* what
 
 void check_mem_kind(int mk) { need(mk == PGGC_MEM_HOST || mk == PGGC_MEM_DEVICE, "mem_kind must be PGGC_MEM_HOST or PGGC_MEM_DEVICE"); }
 
+// CSR checks on the device copy: bit 0 bad offsets, bit 1 column out of range,
+// bit 2 self-loop.  Columns are only checked inside well-formed rows.
+__global__ void k_validate_csr(const i64* rowptr, const i32* col, i64 n, i64 nnz, int* bad) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        i64 b = rowptr[i], e = rowptr[i + 1];
+        if (b < 0 || e < b || e > nnz || (i == 0 && b != 0) || (i == n - 1 && e != nnz)) {
+            atomicOr(bad, 1);
+            continue;
+        }
+        for (i64 j = b; j < e; j++) {
+            i32 v = col[j];
+            if (v < 0 || v >= n) atomicOr(bad, 2);
+            else if (v == (i32)i) atomicOr(bad, 4);
+        }
+    }
+}
+
+void validate_csr_device(Context& c, const i64* rowptr, const i32* col, i64 n, i64 nnz) {
+    DBuf<int> bad(c, 1);
+    PGGC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), c.stream));
+    if (n > 0) {
+        k_validate_csr<<<(int)std::min<i64>(ceil_div(n, 256), (i64)c.num_sms * 16), 256, 0, c.stream>>>(rowptr, col, n,
+                                                                                                       nnz, bad.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    int b = c.read1(bad.p);
+    if (n == 0) {
+        i64 r0 = c.read1(rowptr);
+        need(r0 == 0 && nnz == 0, "an empty graph must have rowptr = {0} and nnz = 0");
+    }
+    need(!(b & 1), "rowptr must start at 0, be non-decreasing and end at nnz");
+    need(!(b & 2), "column index out of range");
+    need(!(b & 4), "self-loops are not supported");
+}
+
 template <class W>
 std::unique_ptr<Graph<W>> make_graph(Context& ctx, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col,
                                      const void* weights, int kind, const void* vtx_w, int objective, int mem_kind) {
@@ -126,6 +165,7 @@ std::unique_ptr<Graph<W>> make_graph(Context& ctx, int64_t n, int64_t nnz, const
     auto kindc = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     PGGC_CUDA(cudaMemcpyAsync(g->rowptr.p, rowptr, sizeof(i64) * (n + 1), kindc, ctx.stream));
     if (nnz > 0) PGGC_CUDA(cudaMemcpyAsync(g->col.p, col, sizeof(i32) * nnz, kindc, ctx.stream));
+    validate_csr_device(ctx, g->rowptr.p, g->col.p, n, nnz);
     if (!g->uniform) {
         need(weights != nullptr, "weights required for a non-uniform graph");
         g->w = DBuf<W>(ctx, std::max<i64>(nnz, 1));
@@ -139,18 +179,6 @@ std::unique_ptr<Graph<W>> make_graph(Context& ctx, int64_t n, int64_t nnz, const
     }
     ctx.sync();
     return g;
-}
-
-void validate_csr_host(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col) {
-    need(rowptr[0] == 0, "rowptr[0] must be 0");
-    need(rowptr[n] == nnz, "rowptr[n] must equal nnz");
-    for (int64_t i = 0; i < n; i++) {
-        need(rowptr[i + 1] >= rowptr[i], "rowptr must be non-decreasing");
-        for (int64_t j = rowptr[i]; j < rowptr[i + 1]; j++) {
-            need(col[j] >= 0 && col[j] < n, "column index out of range");
-            need(col[j] != i, "self-loops are not supported");
-        }
-    }
 }
 
 template <class F>
@@ -204,6 +232,36 @@ struct I64Arr {
 extern "C" {
 
 const char* pggc_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t pggc_launch_count(void) { return (uint64_t)pggc::g_kernel_launches.load(); }
+
+pggc_status pggc_profile_enable(pggc_context* ctx, int on) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL context");
+        ctx->ctx->prof_flush();
+        ctx->ctx->profiling = on != 0;
+    });
+}
+
+pggc_status pggc_profile_reset(pggc_context* ctx) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL context");
+        ctx->ctx->prof_reset();
+    });
+}
+
+pggc_status pggc_profile_read(pggc_context* ctx, const char* family, int64_t* launches, double* ms, double* bytes) {
+    return guarded([&] {
+        need(ctx && family, "NULL argument");
+        ctx->ctx->prof_flush();
+        auto it = ctx->ctx->prof.find(family);
+        ProfStat st;
+        if (it != ctx->ctx->prof.end()) st = it->second;
+        if (launches) *launches = st.launches;
+        if (ms) *ms = st.ms;
+        if (bytes) *bytes = st.bytes;
+    });
+}
 const char* pggc_version(void) { return "pggc-b200 0.1 sm_100a"; }
 
 pggc_status pggc_context_create(int device, pggc_context** out) {
@@ -244,7 +302,6 @@ pggc_status pggc_graph_create(pggc_context* ctx, int64_t n, int64_t nnz, const i
         need(weight_kind >= PGGC_W_UNIFORM && weight_kind <= PGGC_W_FLOAT32, "unknown weight kind");
         need(objective >= PGGC_OBJ_MOD && objective <= PGGC_OBJ_LCC, "unknown objective");
         check_mem_kind(mem_kind);
-        if (mem_kind == PGGC_MEM_HOST) validate_csr_host(n, nnz, rowptr, col);
         Context& c = *ctx->ctx;
         c.sync();
         auto* g = new pggc_graph();
@@ -648,7 +705,10 @@ pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const 
             In<i32> lab(c, labels, n, mem_kind);
             DBuf<int> bad(c, 1);
             PGGC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), c.stream));
-            if (n > 0) k_check_labels<<<(int)std::min<i64>(ceil_div(n, 256), 4096), 256, 0, c.stream>>>(lab.p, n, bad.p);
+            if (n > 0) {
+                k_check_labels<<<(int)std::min<i64>(ceil_div(n, 256), 4096), 256, 0, c.stream>>>(lab.p, n, bad.p);
+                PGGC_LAUNCH_CHECK();
+            }
             need(c.read1(bad.p) == 0, "labels must lie in [0, n)");
             ClusterState<V> cs;
             make_cluster_state<W>(c, gr, objective, lambda_mult, cs);

@@ -12,6 +12,7 @@
 //    applied recursively to group totals.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <limits>
@@ -65,7 +66,14 @@ struct DeviceFault : std::runtime_error {
                                                        __FILE__ + ":" + std::to_string(__LINE__)); \
     } while (0)
 
-#define PGGC_LAUNCH_CHECK() PGGC_CUDA(cudaGetLastError())
+// Every kernel launch is followed by exactly one PGGC_LAUNCH_CHECK(), which also
+// counts the launch (pggc_launch_count()).
+extern std::atomic<unsigned long long> g_kernel_launches;
+#define PGGC_LAUNCH_CHECK()                                                        \
+    do {                                                                           \
+        PGGC_CUDA(cudaGetLastError());                                             \
+        ::pggc::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);         \
+    } while (0)
 
 template <class W> struct Traits;
 template <> struct Traits<i32> { using V = i64; };

@@ -3,9 +3,20 @@
 // allocations from the device memory pool, pinned host scalars for the few
 // values the host must read, and a device error flag latched by bounded loops.
 #pragma once
+#include <map>
+#include <vector>
 #include "common.cuh"
 
 namespace pggc {
+
+// Per-kernel-family timing with CUDA events on the launching stream, plus the
+// algorithmic bytes the kernels report (accumulated on the device per warp and
+// flushed with one atomic per warp).  Off unless enabled.
+struct ProfStat {
+    i64 launches = 0;
+    double ms = 0.0;
+    double bytes = 0.0;
+};
 
 struct Context {
     int device = 0;
@@ -15,6 +26,13 @@ struct Context {
     size_t h_pin_bytes = 0;
     int num_sms = NUM_SMS;
     size_t max_smem_optin = 0;
+    // profiling
+    bool profiling = false;
+    unsigned long long* d_prof = nullptr;  // [64] device byte counters
+    std::map<std::string, int> prof_slot;
+    std::map<std::string, ProfStat> prof;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    std::vector<cudaEvent_t> ev_pool;
 
     explicit Context(int dev) : device(dev) {
         PGGC_CUDA(cudaSetDevice(dev));
@@ -25,6 +43,8 @@ struct Context {
         PGGC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
         PGGC_CUDA(cudaMallocAsync((void**)&d_err, sizeof(int) * 8, stream));
         PGGC_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int) * 8, stream));
+        PGGC_CUDA(cudaMallocAsync((void**)&d_prof, sizeof(unsigned long long) * 64, stream));
+        PGGC_CUDA(cudaMemsetAsync(d_prof, 0, sizeof(unsigned long long) * 64, stream));
         h_pin_bytes = 4096;
         PGGC_CUDA(cudaMallocHost(&h_pin, h_pin_bytes));
         cudaDeviceProp prop;
@@ -34,6 +54,13 @@ struct Context {
         PGGC_CUDA(cudaStreamSynchronize(stream));
     }
     ~Context() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& pe : prof_pending) {
+            cudaEventDestroy(pe.second.first);
+            cudaEventDestroy(pe.second.second);
+        }
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        if (d_prof) cudaFreeAsync(d_prof, stream);
         if (d_err) cudaFreeAsync(d_err, stream);
         if (stream) cudaStreamSynchronize(stream);
         if (h_pin) cudaFreeHost(h_pin);
@@ -65,12 +92,86 @@ struct Context {
     T read1(const T* d) {
         return *(T*)readback(d, sizeof(T));
     }
+    // ---- profiling -----------------------------------------------------
+    // device counter slot for a family (nullptr when profiling is off)
+    unsigned long long* prof_counter(const char* family) {
+        if (!profiling) return nullptr;
+        auto it = prof_slot.find(family);
+        int slot;
+        if (it == prof_slot.end()) {
+            slot = (int)prof_slot.size();
+            if (slot >= 64) return nullptr;
+            prof_slot[family] = slot;
+        } else {
+            slot = it->second;
+        }
+        return d_prof + slot;
+    }
+    cudaEvent_t take_event() {
+        if (!ev_pool.empty()) {
+            cudaEvent_t e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        PGGC_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+    void prof_record(const std::string& family, cudaEvent_t a, cudaEvent_t b) {
+        prof_pending.push_back({family, {a, b}});
+        if (prof_pending.size() >= 8192) prof_flush();
+    }
+    void prof_flush() {
+        if (prof_pending.empty() && prof_slot.empty()) return;
+        sync();
+        for (auto& pe : prof_pending) {
+            float ms = 0.f;
+            PGGC_CUDA(cudaEventElapsedTime(&ms, pe.second.first, pe.second.second));
+            auto& st = prof[pe.first];
+            st.launches += 1;
+            st.ms += ms;
+            ev_pool.push_back(pe.second.first);
+            ev_pool.push_back(pe.second.second);
+        }
+        prof_pending.clear();
+        if (!prof_slot.empty()) {
+            unsigned long long h[64];
+            PGGC_CUDA(cudaMemcpy(h, d_prof, sizeof(h), cudaMemcpyDeviceToHost));
+            for (auto& kv : prof_slot) prof[kv.first].bytes += (double)h[kv.second];
+            PGGC_CUDA(cudaMemsetAsync(d_prof, 0, sizeof(h), stream));
+            sync();
+        }
+    }
+    void prof_reset() {
+        prof_flush();
+        prof.clear();
+    }
+
     void check_device_error() {
         int e = read1(d_err);
         if (e != DEV_OK) {
             PGGC_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
             sync();
             throw DeviceFault("device-side bounded loop gave up (code " + std::to_string(e) + ")");
+        }
+    }
+};
+
+// Brackets the launches of one kernel family with CUDA events when profiling.
+struct ProfScope {
+    Context& ctx;
+    const char* family;
+    cudaEvent_t a = nullptr, b = nullptr;
+    ProfScope(Context& c, const char* f) : ctx(c), family(f) {
+        if (ctx.profiling) {
+            a = ctx.take_event();
+            PGGC_CUDA(cudaEventRecord(a, ctx.stream));
+        }
+    }
+    ~ProfScope() {
+        if (a) {
+            b = ctx.take_event();
+            if (cudaEventRecord(b, ctx.stream) == cudaSuccess) ctx.prof_record(family, a, b);
         }
     }
 };

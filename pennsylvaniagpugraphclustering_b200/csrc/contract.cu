@@ -378,6 +378,7 @@ struct ListUIn {
 template <class W>
 std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, const i32* vcmap, i64 nc) {
     using V = typename Traits<W>::V;
+    ProfScope ps(ctx, "contract");
     auto cg = std::make_unique<Graph<W>>();
     cg->n = nc;
     cg->uniform = false;

@@ -184,6 +184,10 @@ __global__ void k_project(i64 n, i32* fine, const i32* coarse) {
     for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n; x += (i64)gridDim.x * blockDim.x)
         fine[x] = coarse[fine[x]];
 }
+// The reference's level loop has no bound (src/clustering_methods.cpp:59,147);
+// a hierarchy this deep means the refinement stopped contracting.
+constexpr i64 MAX_LEVELS = 4096;
+
 inline int vgrid(Context& ctx, i64 n) { return (int)std::max<i64>(1, std::min<i64>(ceil_div(n, 256), (i64)ctx.num_sms * 16)); }
 
 // leiden_part<plus,improve> (src/clustering_methods.cpp:47-137)
@@ -203,6 +207,7 @@ void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits
     MoveStats ms;
     while (true) {
         const Graph<W>& c = *levels.back();
+        if ((i64)levels.size() > MAX_LEVELS) throw DeviceFault("multilevel hierarchy exceeded MAX_LEVELS");
         double old_obj = rfd.obj;
         bool init = !improve && levels.size() == 1;
         generate_orderings(ctx, c.view().rowptr, c.n, ord);
@@ -281,6 +286,7 @@ void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Trait
     MoveStats ms;
     while (true) {
         const Graph<W>& c = *levels.back();
+        if ((i64)levels.size() > MAX_LEVELS) throw DeviceFault("multilevel hierarchy exceeded MAX_LEVELS");
         DBuf<i32> part(ctx, std::max<i64>(c.n, 1));
         iota<i32>(ctx, part.p, c.n);
         generate_orderings(ctx, c.view().rowptr, c.n, ord);

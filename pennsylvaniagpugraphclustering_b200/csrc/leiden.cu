@@ -460,6 +460,7 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     using V = typename Traits<W>::V;
     const i64 n = g.n;
     if (n == 0) return 0;
+    ProfScope ps(ctx, "leiden_refine");
     auto gv = g.view();
     const float gamma = (float)cs.lambda;
     const int grid = (int)std::min<i64>(ceil_div(n, 256), (i64)ctx.num_sms * 16);
@@ -477,18 +478,33 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     DBuf<i32> hn(ctx, n), order(ctx, n), vcmap(ctx, n);
     PickArgs<W> pa{gv, constraint, well.p, gamma, seed_pick, hn.p};
     if (g.uniform) {
-        if (nsmall > 0) k_pick_uniform_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list, nsmall);
-        if (nmass > 0) k_pick_uniform_block<W><<<gb, 1024, 0, ctx.stream>>>(pa, mass_list, nmass);
+        if (nsmall > 0) {
+            k_pick_uniform_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list, nsmall);
+            PGGC_LAUNCH_CHECK();
+        }
+        if (nmass > 0) {
+            k_pick_uniform_block<W><<<gb, 1024, 0, ctx.stream>>>(pa, mass_list, nmass);
+            PGGC_LAUNCH_CHECK();
+        }
     } else {
-        if (nsmall > 0) k_pick_heavy_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list, nsmall);
-        if (nmass > 0) k_pick_heavy_block<W><<<gb, 1024, 0, ctx.stream>>>(pa, mass_list, nmass);
+        if (nsmall > 0) {
+            k_pick_heavy_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list, nsmall);
+            PGGC_LAUNCH_CHECK();
+        }
+        if (nmass > 0) {
+            k_pick_heavy_block<W><<<gb, 1024, 0, ctx.stream>>>(pa, mass_list, nmass);
+            PGGC_LAUNCH_CHECK();
+        }
     }
-    PGGC_LAUNCH_CHECK();
     k_set_order<<<grid, 256, 0, ctx.stream>>>(n, seed_order, order.p);
+    PGGC_LAUNCH_CHECK();
     k_unselect<<<grid, 256, 0, ctx.stream>>>(n, order.p, hn.p);
+    PGGC_LAUNCH_CHECK();
     fill<i32>(ctx, vcmap.p, n, ORD_MAX);
     k_trees_part1<<<grid, 256, 0, ctx.stream>>>(n, hn.p, order.p, vcmap.p, ctx.d_err);
+    PGGC_LAUNCH_CHECK();
     k_trees_flip<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, order.p);
+    PGGC_LAUNCH_CHECK();
     k_trees_part2<<<grid, 256, 0, ctx.stream>>>(n, hn.p, order.p, vcmap.p, ctx.d_err);
     PGGC_LAUNCH_CHECK();
 
@@ -512,9 +528,14 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
         k_shift_excl<<<grid, 256, 0, ctx.stream>>>(n, inc.p, ts.p);
         PGGC_LAUNCH_CHECK();
     }
-    if (nsmall > 0) k_inner_warp<W><<<gw, 256, 0, ctx.stream>>>(gv, small_list, nsmall, vcmap.p, order.p, inner.p);
-    if (nmass > 0) k_inner_block<W><<<gb, 1024, 0, ctx.stream>>>(gv, mass_list, nmass, vcmap.p, order.p, inner.p);
-    PGGC_LAUNCH_CHECK();
+    if (nsmall > 0) {
+        k_inner_warp<W><<<gw, 256, 0, ctx.stream>>>(gv, small_list, nsmall, vcmap.p, order.p, inner.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    if (nmass > 0) {
+        k_inner_block<W><<<gb, 1024, 0, ctx.stream>>>(gv, mass_list, nmass, vcmap.p, order.p, inner.p);
+        PGGC_LAUNCH_CHECK();
+    }
     DBuf<long long> breakers(ctx, n);
     fill<long long>(ctx, breakers.p, n, (long long)n);
     GammaArgs<W> ga{n, ids.p, vcmap.p, row_map.p, ts.p, inner.p, oc.p, g.vtx_w.p, cs.total_deg.p, constraint, gamma,
@@ -530,6 +551,7 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
         PGGC_LAUNCH_CHECK();
     }
     k_break_part2<W><<<grid, 256, 0, ctx.stream>>>(ga);
+    PGGC_LAUNCH_CHECK();
     k_break_apply<<<grid, 256, 0, ctx.stream>>>(n, ids.p, breakers.p, vcmap.p);
     PGGC_LAUNCH_CHECK();
 

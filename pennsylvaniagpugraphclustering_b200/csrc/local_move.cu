@@ -66,7 +66,18 @@ struct SelArgs {
     float fr;
     int initial;
     int* err;
+    unsigned long long* prof;  // algorithmic-byte counter (profiling only)
 };
+
+// algorithmic bytes of one select evaluation: list entry + dest read, then
+// rowptr pair, vtx_w, part, pval, D[part], dest/gain writes, and per edge the
+// column, weight and neighbour label (initial mode: column, weight, D[v])
+template <class W>
+__device__ __forceinline__ unsigned long long sel_bytes(const SelArgs<W>& a, i64 deg, bool evaluated) {
+    if (!evaluated) return 8;
+    const unsigned long long wb = a.g.w ? sizeof(W) : 0;
+    return 60ull + (unsigned long long)deg * (a.initial ? (12ull + wb) : (8ull + wb));
+}
 
 struct VCtx {
     i32 p;
@@ -183,11 +194,16 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, c
     const int l = lane_id(), w = threadIdx.x >> 5;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    unsigned long long pb = 0;
     for (i64 x = gw; x < count; x += nw) {
         i32 i = list[x];
-        if (a.dest[i] == NO_MOVE) continue;
+        if (a.dest[i] == NO_MOVE) {
+            pb += sel_bytes(a, 0, false);
+            continue;
+        }
         VCtx vc = sel_prologue(a, i);
         i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        pb += sel_bytes(a, e - b, true);
         Best best = none_best();
         if (a.initial) {
             for (i64 j = b + l; j < e; j += 32) sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
@@ -222,6 +238,7 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, c
         warp_best(best);
         if (l == 0) sel_finish(a, i, vc, best);
     }
+    if (a.prof && l == 0 && pb) atomicAdd(a.prof, pb);
 }
 
 // ---- block per vertex (256 threads), shared or global table ----------------
@@ -236,11 +253,16 @@ __global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* l
     const int l = lane_id(), w = threadIdx.x >> 5;
     i32* keys = GLOBAL ? gkeys + (i64)blockIdx.x * gcap : skeys;
     V* vals = GLOBAL ? gvals + (i64)blockIdx.x * gcap : svals;
+    unsigned long long pb = 0;
     for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
         i32 i = list[x];
         i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
         if (!GLOBAL && e - b > HUGE_DEG) continue;
-        if (a.dest[i] == NO_MOVE) continue;
+        if (a.dest[i] == NO_MOVE) {
+            pb += sel_bytes(a, 0, false);
+            continue;
+        }
+        pb += sel_bytes(a, e - b, true);
         VCtx vc = sel_prologue(a, i);
         Best best = none_best();
         if (a.initial) {
@@ -270,6 +292,7 @@ __global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* l
         }
         __syncthreads();
     }
+    if (a.prof && threadIdx.x == 0 && pb) atomicAdd(a.prof, pb);
 }
 
 // ---------------------------------------------------------------------------
@@ -364,6 +387,7 @@ void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, cons
                       typename Traits<W>::V* out, int mode, unsigned char* flags, i32* dest) {
     auto gv = g.view();
     if (g.n == 0) return;
+    ProfScope ps(ctx, "own_weights");
     int grid = (int)std::min<i64>(ceil_div(ceil_div(g.n, 32), 8), (i64)ctx.num_sms * 16);
     k_own_warp<W><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, mode, flags, dest);
     PGGC_LAUNCH_CHECK();
@@ -395,7 +419,16 @@ struct ABArgs {
     const i32* cand;
     unsigned char* keep;
     const LMScalars<V>* sc;
+    unsigned long long* prof;
 };
+
+// algorithmic bytes of one afterburner evaluation: candidate entry, its
+// dest/part/vtx_w/gain, rowptr pair, keep flag; per edge column, weight, gain[v]
+template <class W>
+__device__ __forceinline__ unsigned long long ab_bytes(const ABArgs<W>& a, i64 deg) {
+    const unsigned long long wb = a.g.w ? sizeof(W) : 0;
+    return 41ull + (unsigned long long)deg * (8ull + wb);
+}
 
 template <class W>
 __device__ __forceinline__ double ab_term(const ABArgs<W>& a, i64 j, i32 p, i32 best, float multi, float igain,
@@ -422,16 +455,19 @@ __global__ void __launch_bounds__(256) k_afterburner_warp(ABArgs<W> a) {
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
     const i64 hi_x = a.sc->split;
+    unsigned long long pb = 0;
     for (i64 x = gw; x < hi_x; x += nw) {
         i32 i = a.cand[x];
         i32 best = a.dest[i], p = a.part[i];
         float multi = to_f(a.g.vtx_w[i]) * a.pm;
         float igain = a.gain[i];
         i32 hi = (i32)xorshift32((u32)i);
+        pb += ab_bytes(a, a.g.rowptr[i + 1] - a.g.rowptr[i]);
         double ch = warp_canon_sum(a.g.rowptr[i], a.g.rowptr[i + 1],
                                    [&](i64 j) { return ab_term(a, j, p, best, multi, igain, hi); });
         if (lane_id() == 0) a.keep[x] = (igain + (float)ch) >= 0.0f ? 1 : 0;
     }
+    if (a.prof && lane_id() == 0 && pb) atomicAdd(a.prof, pb);
 }
 
 template <class W>
@@ -894,18 +930,23 @@ struct Mover {
         a.fr = fr;
         a.initial = initial ? 1 : 0;
         a.err = ctx.d_err;
+        a.prof = nullptr;
         return a;
     }
 
     template <bool CON>
-    void launch_select_t(const SelArgs<W>& a) {
+    void launch_select_t(SelArgs<W> a) {
         if (ord.off_large > 0) {
+            ProfScope ps(ctx, "select_warp");
+            a.prof = ctx.prof_counter("select_warp");
             int grid = grid_for(ctx, ceil_div(ord.off_large, SELW_WARPS), 1, 16);
             k_select_warp<W, CON><<<grid, SELW_WARPS * 32, 0, ctx.stream>>>(a, ord.order1.p, ord.off_large);
             PGGC_LAUNCH_CHECK();
         }
         i64 nb = n - ord.off_large;
         if (nb > 0) {
+            ProfScope ps(ctx, "select_block");
+            a.prof = ctx.prof_counter("select_block");
             size_t sm = (sizeof(V) + sizeof(i32)) * SEL_TS_MAX;
             PGGC_CUDA(cudaFuncSetAttribute(k_select_block<W, CON, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)sm));
@@ -915,6 +956,8 @@ struct Mover {
             PGGC_LAUNCH_CHECK();
         }
         if (ord.n_huge > 0) {
+            ProfScope ps(ctx, "select_huge");
+            a.prof = ctx.prof_counter("select_huge");
             int grid = (int)std::min<i64>(ord.n_huge, 32);
             k_select_block<W, CON, true><<<grid, 256, 0, ctx.stream>>>(a, ord.huge.p, ord.n_huge, gkeys.p, gvals.p, gcap);
             PGGC_LAUNCH_CHECK();
@@ -947,11 +990,17 @@ struct Mover {
         a.cand = cand.p;
         a.keep = keep.p;
         a.sc = sc.p;
+        a.prof = ctx.prof_counter("afterburner_warp");
         int grid = grid_for(ctx, ceil_div(n, 8), 1, 16);
-        k_afterburner_warp<W><<<grid, 256, 0, ctx.stream>>>(a);
-        PGGC_LAUNCH_CHECK();
+        {
+            ProfScope ps(ctx, "afterburner_warp");
+            k_afterburner_warp<W><<<grid, 256, 0, ctx.stream>>>(a);
+            PGGC_LAUNCH_CHECK();
+        }
         i64 nm = n - ord.off_large2;
         if (nm > 0) {
+            ProfScope ps(ctx, "afterburner_block");
+            a.prof = nullptr;
             k_afterburner_block<W><<<(int)std::min<i64>(nm, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(a);
             PGGC_LAUNCH_CHECK();
         }
@@ -1043,6 +1092,7 @@ struct Mover {
         radix_sort_pairs<i32>(ctx, kp.p, op.p, k, 32, 64, kt.p, ot.p);
         DBuf<V> wd(ctx, k), wp(ctx, k), Ed(ctx, k + 1), Ep(ctx, k + 1);
         k_gather_vw<V><<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(od.p, moves.p, g.vtx_w.p, k, wd.p);
+        PGGC_LAUNCH_CHECK();
         k_gather_vw<V><<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(op.p, moves.p, g.vtx_w.p, k, wp.p);
         PGGC_LAUNCH_CHECK();
         if constexpr (std::is_same<V, i64>::value) {

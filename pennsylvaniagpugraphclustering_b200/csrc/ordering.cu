@@ -96,6 +96,7 @@ void generate_orderings(Context& ctx, const i64* rowptr, i64 n, Ordering& o) {
         o.off_large = o.off_large2 = o.off_mid = o.off_mid2 = o.max_deg = o.n_huge = 0;
         return;
     }
+    ProfScope ps(ctx, "orderings");
     i64 nb = ceil_div(n, ORD_THREADS);
     DBuf<i64> cnt1(ctx, 3 * nb), cnt2(ctx, 3 * nb), scal(ctx, 8);
     PGGC_CUDA(cudaMemsetAsync(scal.p, 0, 8 * sizeof(i64), ctx.stream));
