@@ -67,6 +67,12 @@ const char* pggc_version(void);
 /* kernels launched by this library in this process so far */
 uint64_t pggc_launch_count(void);
 
+/* Fault injection for tests: cap every hash-table probe sequence at `limit`
+ * probes (0 restores the default bound, the table size).  A capped probe that
+ * gives up latches a device error and the call returns PGGC_ERR_DEVICE; the
+ * context stays usable. */
+pggc_status pggc_debug_set_probe_limit(pggc_context* ctx, int limit);
+
 /* Per-kernel-family timing (CUDA events on the context stream) and algorithmic
  * byte counts, for roofline reporting; the counterpart of the reference's
  * EXTRA_TIMING measurements (src/clustering_methods.cpp:78-108).  Families:

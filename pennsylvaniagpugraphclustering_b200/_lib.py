@@ -50,6 +50,7 @@ _SIGS = {
     "pggc_last_error": (ctypes.c_char_p, []),
     "pggc_version": (ctypes.c_char_p, []),
     "pggc_launch_count": (_u64, []),
+    "pggc_debug_set_probe_limit": (_ci, [_vp, _ci]),
     "pggc_profile_enable": (_ci, [_vp, _ci]),
     "pggc_profile_reset": (_ci, [_vp]),
     "pggc_profile_read": (_ci, [_vp, ctypes.c_char_p, ctypes.POINTER(_i64), ctypes.POINTER(_dbl),

@@ -235,6 +235,14 @@ const char* pggc_last_error(void) { return g_last_error.c_str(); }
 
 uint64_t pggc_launch_count(void) { return (uint64_t)pggc::g_kernel_launches.load(); }
 
+pggc_status pggc_debug_set_probe_limit(pggc_context* ctx, int limit) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL context");
+        need(limit >= 0, "limit must be >= 0");
+        ctx->ctx->probe_cap = (u32)limit;
+    });
+}
+
 pggc_status pggc_profile_enable(pggc_context* ctx, int on) {
     return guarded([&] {
         need(ctx != nullptr, "NULL context");

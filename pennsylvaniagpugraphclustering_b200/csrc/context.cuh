@@ -26,6 +26,8 @@ struct Context {
     size_t h_pin_bytes = 0;
     int num_sms = NUM_SMS;
     size_t max_smem_optin = 0;
+    // fault injection: cap on hash-table probes (0 = only the table size bounds them)
+    u32 probe_cap = 0;
     // profiling
     bool profiling = false;
     unsigned long long* d_prof = nullptr;  // [64] device byte counters

@@ -63,6 +63,7 @@ struct CArgs {
     V* out_val;
     i64* ucount;         // unique neighbours per coarse vertex
     int* err;
+    u32 probe_cap;       // fault-injection cap on hash probes (0: none)
 };
 
 // Edge position j of virtual edge q (global flat index) of coarse vertex c.
@@ -78,10 +79,11 @@ __device__ __forceinline__ i64 flat_edge(const i64* P, const i32* members, const
 }
 
 template <class V>
-__device__ __forceinline__ void ctable_add(i32* keys, V* vals, u32 mask, i32 c, V x, int* err) {
+__device__ __forceinline__ void ctable_add(i32* keys, V* vals, u32 mask, i32 c, V x, int* err, u32 cap) {
     u32 s = xorshift32((u32)c) & mask;
     volatile i32* vk = keys;
-    for (u32 probe = 0; probe <= mask; probe++) {
+    const u32 limit = (cap != 0 && cap <= mask) ? cap : mask + 1;
+    for (u32 probe = 0; probe < limit; probe++) {
         i32 k = vk[s];
         if (k == c) {
             cvatomic_add(&vals[s], x);
@@ -136,7 +138,7 @@ __device__ __forceinline__ void cchunk(const CArgs<W>& a, i32 c, i64 m0, i64 m1,
     unsigned peers = __match_any_sync(FULL, key);
     bool leader = keep && ((peers & lanemask_lt()) == 0);
     V s = a.g.w ? cgroup_sum<V>(peers, wv, leader) : V(__popc(peers));
-    if (leader) ctable_add(keys, vals, mask, u, s, a.err);
+    if (leader) ctable_add(keys, vals, mask, u, s, a.err, a.probe_cap);
 }
 
 constexpr int CW_WARPS = 8;
@@ -432,6 +434,7 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     a.out_val = oval.p;
     a.ucount = ucount.p;
     a.err = ctx.d_err;
+    a.probe_cap = ctx.probe_cap;
     if (n_w > 0) {
         int grid = (int)std::min<i64>(ceil_div(n_w, CW_WARPS), (i64)ctx.num_sms * 8);
         k_contract_warp<W><<<grid, CW_WARPS * 32, 0, ctx.stream>>>(a, lw.p, counts.p + 0);

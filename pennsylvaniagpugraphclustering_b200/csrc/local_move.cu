@@ -67,6 +67,7 @@ struct SelArgs {
     int initial;
     int* err;
     unsigned long long* prof;  // algorithmic-byte counter (profiling only)
+    u32 probe_cap;             // fault-injection cap on hash probes (0: none)
 };
 
 // algorithmic bytes of one select evaluation: list entry + dest read, then
@@ -143,11 +144,14 @@ __device__ __forceinline__ V group_sum(unsigned peers, V val, bool leader) {
     return s;
 }
 
+// Linear-probing insert; gives up (latching DEV_ERR_PROBE) after the table size
+// or `cap` probes, whichever is smaller (cap = 0: no extra limit).
 template <class V>
-__device__ __forceinline__ void table_add(i32* keys, V* vals, u32 mask, i32 c, V x, int* err) {
+__device__ __forceinline__ void table_add(i32* keys, V* vals, u32 mask, i32 c, V x, int* err, u32 cap) {
     u32 s = xorshift32((u32)c) & mask;
     volatile i32* vk = keys;
-    for (u32 probe = 0; probe <= mask; probe++) {
+    const u32 limit = (cap != 0 && cap <= mask) ? cap : mask + 1;
+    for (u32 probe = 0; probe < limit; probe++) {
         i32 k = vk[s];
         if (k == c) {
             vatomic_add(&vals[s], x);
@@ -179,7 +183,7 @@ __device__ __forceinline__ void chunk_to_table(const SelArgs<W>& a, const VCtx& 
     unsigned peers = __match_any_sync(FULL, key);
     bool leader = keep && ((peers & lanemask_lt()) == 0);
     V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
-    if (leader) table_add(keys, vals, mask, c, s, a.err);
+    if (leader) table_add(keys, vals, mask, c, s, a.err, a.probe_cap);
 }
 
 // ---- warp per vertex, degree < 128 (order1 bucket 0) ----------------------
@@ -931,6 +935,7 @@ struct Mover {
         a.initial = initial ? 1 : 0;
         a.err = ctx.d_err;
         a.prof = nullptr;
+        a.probe_cap = ctx.probe_cap;
         return a;
     }
 
