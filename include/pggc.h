@@ -133,10 +133,11 @@ pggc_status pggc_local_move(pggc_context* ctx, const pggc_graph* g, pggc_cluster
 
 /* One candidates_and_destinations pass (src/local_mover.cpp:567-634) on a given
  * state: dest_io is the dest cache in, destinations out (NO_MOVE = -3,
- * NEW_PART = -4); gain_out receives save_gains.  pvals: own-cluster weights
+ * NEW_PART = -4); gain_io is save_gains in/out (skipped NO_MOVE vertices keep
+ * their entries, as src/local_mover.cpp:477-479 does).  pvals: own-cluster weights
  * (V type).  initial != 0 uses the input graph as the conn graph. */
 pggc_status pggc_select_pass(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, const int32_t* part,
-                             const void* pvals, int32_t* dest_io, float* gain_out, float filter_ratio, int initial,
+                             const void* pvals, int32_t* dest_io, float* gain_io, float filter_ratio, int initial,
                              int constrained, const int32_t* constraint, int mem_kind, int64_t* num_candidates);
 
 /* ---- contracter::build_coarse_graph (src/header/contract.h:20-24) --------

@@ -163,11 +163,12 @@ def build_coarse_graph(g: Graph, vcmap, nc) -> Graph:
     return Graph(None, None, _handle=h)
 
 
-def select(g: Graph, cd: ClusterData, part, pvals, dest, filter_ratio, initial, constrained=False, constraint=None):
+def select(g: Graph, cd: ClusterData, part, pvals, dest, filter_ratio, initial, constrained=False, constraint=None,
+           gain=None):
     part = np.ascontiguousarray(part, np.int32)
     pvals = np.ascontiguousarray(pvals, np.float64 if g.wkind == W_FLOAT32 else np.int64)
     dest = np.array(dest, np.int32, copy=True)
-    gain = np.empty(g.n, np.float32)
+    gain = np.zeros(g.n, np.float32) if gain is None else np.array(gain, np.float32, copy=True)
     con = None if constraint is None else np.ascontiguousarray(constraint, np.int32)
     k = lib().orc_select(g.h, cd.h, _p(part), _p(pvals), _p(dest), _p(gain), filter_ratio, int(initial),
                          int(constrained), _p(con))

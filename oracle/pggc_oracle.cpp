@@ -1424,8 +1424,9 @@ void* orc_build_coarse_graph(void* gh, const int32_t* vcmap, int64_t nc) {
 }
 
 // One select pass (candidates_and_destinations) on a given state.
-// dest_io: dest cache in / destinations out; gain_out: save_gains.
-int64_t orc_select(void* gh, void* cdh, const int32_t* part, const void* pvals, int32_t* dest_io, float* gain_out,
+// dest_io: dest cache in / destinations out; gain_io: save_gains in/out (entries
+// of skipped NO_MOVE vertices keep their input values, as save_gains does).
+int64_t orc_select(void* gh, void* cdh, const int32_t* part, const void* pvals, int32_t* dest_io, float* gain_io,
                    float filter_ratio, int initial, int constrained, const int32_t* constraint) {
     auto* g = (OrcGraph*)gh;
     auto* cd = (OrcCD*)cdh;
@@ -1435,13 +1436,13 @@ int64_t orc_select(void* gh, void* cdh, const int32_t* part, const void* pvals, 
         eng.ord = generate_orderings(gg.rowptr.data(), n);
         eng.part.assign(part, part + n);
         eng.dest.assign(dest_io, dest_io + n);
-        eng.gain.assign(n, 0.0f);
+        eng.gain.assign(gain_io, gain_io + n);
         eng.pvals.assign((const V*)pvals, (const V*)pvals + n);
         eng.cdata_init = !initial;
         std::vector<i32> cand;
         eng.select(gg, c, filter_ratio, constrained != 0, constraint, cand);
         std::copy(eng.dest.begin(), eng.dest.end(), dest_io);
-        std::copy(eng.gain.begin(), eng.gain.end(), gain_out);
+        std::copy(eng.gain.begin(), eng.gain.end(), gain_io);
         return (int64_t)cand.size();
     };
     if (g->kind == 2) {

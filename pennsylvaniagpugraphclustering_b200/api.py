@@ -303,10 +303,13 @@ def _local_move(mem, g, part, rfd, is_initial, constraint, sa, strict, sweep_lim
     return _stats_dict(st)
 
 
-def select_pass(mem, g, rfd, part, pvals, dest, filter_ratio, initial, constraint=None):
-    """One candidates_and_destinations pass; returns (dest, gain, num_candidates)."""
+def select_pass(mem, g, rfd, part, pvals, dest, filter_ratio, initial, constraint=None, gain=None):
+    """One candidates_and_destinations pass; returns (dest, gain, num_candidates).
+
+    ``gain`` is save_gains in/out (zeros when omitted): vertices skipped by the
+    dest cache keep their entries."""
     dest = np.array(dest, np.int32, copy=True)
-    gain = np.empty(g.n, np.float32)
+    gain = np.zeros(g.n, np.float32) if gain is None else np.array(gain, np.float32, copy=True)
     pp, _, a1 = _ptr(part, np.int32)
     vp, _, a2 = _ptr(pvals, g.vdtype)
     cp, _, a3 = _ptr(constraint, np.int32) if constraint is not None else (None, None, None)

@@ -10,9 +10,18 @@ namespace pggc {
 std::atomic<unsigned long long> g_kernel_launches{0};
 }
 
+// The context is reference counted: every graph and cluster_data created on it
+// holds a reference, so the device buffers they own are released on a live
+// stream whatever order the caller destroys things in.
 struct pggc_context {
     std::unique_ptr<Context> ctx;
+    std::atomic<int> refs{1};
 };
+
+static void ctx_retain(pggc_context* c) { c->refs.fetch_add(1); }
+static void ctx_release(pggc_context* c) {
+    if (c && c->refs.fetch_sub(1) == 1) delete c;
+}
 
 struct pggc_graph {
     pggc_context* owner = nullptr;
@@ -20,12 +29,25 @@ struct pggc_graph {
     std::unique_ptr<Graph<i32>> gi;
     std::unique_ptr<Graph<float>> gf;
     bool is_float() const { return kind == PGGC_W_FLOAT32; }
+    explicit pggc_graph(pggc_context* o) : owner(o) { ctx_retain(o); }
+    ~pggc_graph() {
+        gi.reset();
+        gf.reset();
+        ctx_release(owner);
+    }
 };
 
 struct pggc_cluster_data {
+    pggc_context* owner = nullptr;
     bool is_float = false;
     ClusterState<i64> ci;
     ClusterState<double> cf;
+    explicit pggc_cluster_data(pggc_context* o) : owner(o) { ctx_retain(o); }
+    ~pggc_cluster_data() {
+        ci.total_deg.reset();
+        cf.total_deg.reset();
+        ctx_release(owner);
+    }
 };
 
 namespace {
@@ -290,7 +312,7 @@ pggc_status pggc_context_create(int device, pggc_context** out) {
 }
 
 pggc_status pggc_context_destroy(pggc_context* ctx) {
-    return guarded([&] { delete ctx; });
+    return guarded([&] { ctx_release(ctx); });
 }
 
 pggc_status pggc_context_stream(pggc_context* ctx, void** stream_out) {
@@ -312,8 +334,7 @@ pggc_status pggc_graph_create(pggc_context* ctx, int64_t n, int64_t nnz, const i
         check_mem_kind(mem_kind);
         Context& c = *ctx->ctx;
         c.sync();
-        auto* g = new pggc_graph();
-        g->owner = ctx;
+        auto* g = new pggc_graph(ctx);
         g->kind = weight_kind;
         try {
             if (weight_kind == PGGC_W_FLOAT32)
@@ -369,7 +390,7 @@ pggc_status pggc_cluster_data_create(pggc_context* ctx, const pggc_graph* g, int
         need(ctx && g && out, "NULL argument");
         need(objective >= PGGC_OBJ_MOD && objective <= PGGC_OBJ_LCC, "unknown objective");
         Context& c = *ctx->ctx;
-        auto* cd = new pggc_cluster_data();
+        auto* cd = new pggc_cluster_data(ctx);
         try {
             cd->is_float = g->is_float();
             if (g->is_float()) make_cluster_state<float>(c, *g->gf, objective, lambda_mult, cd->cf);
@@ -506,10 +527,10 @@ pggc_status pggc_local_move(pggc_context* ctx, const pggc_graph* g, pggc_cluster
 }
 
 pggc_status pggc_select_pass(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, const int32_t* part,
-                             const void* pvals, int32_t* dest_io, float* gain_out, float filter_ratio, int initial,
+                             const void* pvals, int32_t* dest_io, float* gain_io, float filter_ratio, int initial,
                              int constrained, const int32_t* constraint, int mem_kind, int64_t* num_candidates) {
     return guarded([&] {
-        need(ctx && g && cd && part && pvals && dest_io && gain_out, "NULL argument");
+        need(ctx && g && cd && part && pvals && dest_io && gain_io, "NULL argument");
         need(cd->is_float == g->is_float(), "cluster_data / graph weight kinds differ");
         check_mem_kind(mem_kind);
         Context& c = *ctx->ctx;
@@ -527,7 +548,7 @@ pggc_status pggc_select_pass(pggc_context* ctx, const pggc_graph* g, pggc_cluste
             }
             check_labels(c, pin.p, gr.n, cs.label_count, "partition labels must lie in [0, label_count)");
             Out<i32> dest(c, dest_io, gr.n, mem_kind, true);
-            Out<float> gain(c, gain_out, gr.n, mem_kind, false);
+            Out<float> gain(c, gain_io, gr.n, mem_kind, true);
             Ordering o;
             generate_orderings(c, gr.view().rowptr, gr.n, o);
             i64 k = select_pass(c, gr, o, pin.p, pv.p, cs, dest.p, gain.p, filter_ratio, initial != 0,
@@ -546,8 +567,7 @@ pggc_status pggc_build_coarse_graph(pggc_context* ctx, const pggc_graph* g, cons
         need(ctx && g && vcmap && out, "NULL argument");
         check_mem_kind(mem_kind);
         Context& c = *ctx->ctx;
-        auto* cg = new pggc_graph();
-        cg->owner = ctx;
+        auto* cg = new pggc_graph(ctx);
         try {
             dispatch(g, [&](auto& gr, auto* vtag) {
                 using V = std::remove_pointer_t<decltype(vtag)>;

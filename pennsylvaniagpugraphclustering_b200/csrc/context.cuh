@@ -55,8 +55,26 @@ struct Context {
         max_smem_optin = prop.sharedMemPerBlockOptin;
         PGGC_CUDA(cudaStreamSynchronize(stream));
     }
+    // grow-only scratch slots reused across calls (one user at a time per slot)
+    std::vector<std::pair<void*, size_t>> ws;
+    template <class T>
+    T* ws_get(int slot, i64 count) {
+        size_t bytes = sizeof(T) * (size_t)(count > 0 ? count : 1);
+        if (slot >= (int)ws.size()) ws.resize(slot + 1, {nullptr, 0});
+        auto& e = ws[slot];
+        if (e.second < bytes) {
+            if (e.first) PGGC_CUDA(cudaFreeAsync(e.first, stream));
+            size_t nb = bytes + bytes / 4;
+            PGGC_CUDA(cudaMallocAsync(&e.first, nb, stream));
+            e.second = nb;
+        }
+        return (T*)e.first;
+    }
+
     ~Context() {
         if (stream) cudaStreamSynchronize(stream);
+        for (auto& e : ws)
+            if (e.first) cudaFreeAsync(e.first, stream);
         for (auto& pe : prof_pending) {
             cudaEventDestroy(pe.second.first);
             cudaEventDestroy(pe.second.second);

@@ -883,39 +883,47 @@ struct Mover {
     const Ordering& ord;
     i64 n;
     i64 cap;  // label capacity
-    DBuf<i32> part, dest, cand, moves, newl, avail, prio, tmp_i32;
-    DBuf<float> gain;
-    DBuf<V> pvals, pvals_clone, td_curr;
-    DBuf<unsigned char> flags, keep, has;
-    DBuf<LMScalars<V>> sc;
-    DBuf<i32> gkeys;
-    DBuf<V> gvals;
+    // views of context workspace slots (reused across local_move calls)
+    template <class T>
+    struct View {
+        T* p = nullptr;
+    };
+    View<i32> part, dest, cand, moves, newl, avail, prio;
+    View<float> gain;
+    View<V> pvals, pvals_clone, td_curr;
+    View<unsigned char> flags, keep, has;
+    View<LMScalars<V>> sc;
+    View<i32> gkeys;
+    View<V> gvals;
     i64 gcap = 0;
     bool cdata_init = false;
 
+    enum Slot { S_PART, S_DEST, S_CAND, S_MOVES, S_NEWL, S_AVAIL, S_PRIO, S_GAIN, S_PV, S_PVC, S_TD, S_FLAGS, S_KEEP,
+                S_HAS, S_SC, S_GK, S_GV };
+
     Mover(Context& c, const Graph<W>& gr, const Ordering& o, i64 capacity)
         : ctx(c), g(gr), ord(o), n(gr.n), cap(capacity) {
-        i64 nn = std::max<i64>(n, 1);
-        part = DBuf<i32>(ctx, nn);
-        dest = DBuf<i32>(ctx, nn);
-        cand = DBuf<i32>(ctx, nn);
-        moves = DBuf<i32>(ctx, nn);
-        newl = DBuf<i32>(ctx, nn);
-        avail = DBuf<i32>(ctx, std::max<i64>(cap, 1));
-        gain = DBuf<float>(ctx, nn);
-        pvals = DBuf<V>(ctx, nn);
-        pvals_clone = DBuf<V>(ctx, nn);
-        td_curr = DBuf<V>(ctx, std::max<i64>(cap, 1));
-        flags = DBuf<unsigned char>(ctx, nn);
-        keep = DBuf<unsigned char>(ctx, nn);
-        has = DBuf<unsigned char>(ctx, std::max<i64>(cap, 1));
-        sc = DBuf<LMScalars<V>>(ctx, 1);
+        i64 nn = std::max<i64>(n, 1), cc = std::max<i64>(cap, 1);
+        part.p = ctx.ws_get<i32>(S_PART, nn);
+        dest.p = ctx.ws_get<i32>(S_DEST, nn);
+        cand.p = ctx.ws_get<i32>(S_CAND, nn);
+        moves.p = ctx.ws_get<i32>(S_MOVES, nn);
+        newl.p = ctx.ws_get<i32>(S_NEWL, nn);
+        avail.p = ctx.ws_get<i32>(S_AVAIL, cc);
+        gain.p = ctx.ws_get<float>(S_GAIN, nn);
+        pvals.p = ctx.ws_get<V>(S_PV, nn);
+        pvals_clone.p = ctx.ws_get<V>(S_PVC, nn);
+        td_curr.p = ctx.ws_get<V>(S_TD, cc);
+        flags.p = ctx.ws_get<unsigned char>(S_FLAGS, nn);
+        keep.p = ctx.ws_get<unsigned char>(S_KEEP, nn);
+        has.p = ctx.ws_get<unsigned char>(S_HAS, cc);
+        sc.p = ctx.ws_get<LMScalars<V>>(S_SC, 1);
         PGGC_CUDA(cudaMemsetAsync(flags.p, 0, nn, ctx.stream));
         if (ord.n_huge > 0) {
             gcap = next_pow2_u32((u32)std::min<i64>(2 * ord.max_deg, (i64)1 << 30));
             i64 nb = std::min<i64>(ord.n_huge, 32);
-            gkeys = DBuf<i32>(ctx, gcap * nb);
-            gvals = DBuf<V>(ctx, gcap * nb);
+            gkeys.p = ctx.ws_get<i32>(S_GK, gcap * nb);
+            gvals.p = ctx.ws_get<V>(S_GV, gcap * nb);
         }
     }
 
@@ -1073,7 +1081,7 @@ struct Mover {
     // strict prefix selection over moves[0..k); writes sc.num_moves
     void strict_filter(i64 k, i64 split_host, float pm) {
         auto gv = g.view();
-        prio.ensure(ctx, std::max<i64>(n, 1));
+        prio.p = ctx.ws_get<i32>(S_PRIO, std::max<i64>(n, 1));
         fill<i32>(ctx, prio.p, n, (i32)std::min<i64>(n + 1, 2147483647));
         k_prio<<<grid_for(ctx, k, 256), 256, 0, ctx.stream>>>(moves.p, k, prio.p);
         PGGC_LAUNCH_CHECK();

@@ -52,15 +52,29 @@ def test_labels_out_of_range_rejected(mem):
 def test_probe_limit_gives_device_error_and_context_recovers(mem):
     g = G.small_sbm()
     wg = pg.weighted_graph(mem, g.rowptr, g.col)
-    part = np.arange(g.n, dtype=np.int32) // 64  # 64 clusters: many probe collisions
+    # 512 coarse vertices of ~8 scattered members: each hashes ~100 distinct
+    # neighbour ids from [0, 512) into 256 slots, so single-probe inserts collide
+    nc = 512
+    part = ((np.arange(g.n, dtype=np.int64) * 7919) % nc).astype(np.int32)
     cd = pg.get_objective(mem, wg, pg.OBJ_MOD)
     _lib.check(_lib.lib().pggc_debug_set_probe_limit(mem.handle, 1))
     try:
         with pytest.raises(pg.DeviceError):
-            bd = pg.build_coarse_graph(mem, pg.weighted_graph(mem, g.rowptr, g.col), part, 64)
+            pg.build_coarse_graph(mem, wg, part, nc)
     finally:
         _lib.check(_lib.lib().pggc_debug_set_probe_limit(mem.handle, 0))
-    cg = pg.build_coarse_graph(mem, wg, part, 64)
-    assert cg.n == 64 and cg.nnz > 0
+    cg = pg.build_coarse_graph(mem, wg, part, nc)
+    assert cg.n == nc and cg.nnz > 0
     labels, st = pg.run_clustering(mem, wg, cd, method=pg.METHOD_LOUVAIN)
     assert st["label_count"] >= 1
+
+
+def test_destruction_order_is_free(mem):
+    """Graphs and cluster data may outlive the Python context object."""
+    m2 = pg.memory_store(0)
+    g = G.two_cliques()
+    wg = pg.weighted_graph(m2, g.rowptr, g.col)
+    cd = pg.get_objective(m2, wg, pg.OBJ_MOD)
+    m2.close()  # the C context stays alive while wg and cd reference it
+    cd.close()
+    wg.close()

@@ -135,8 +135,10 @@ def test_select_pass(mem, name, fr, initial):
         cd_g.set_state(L, td, uncut)
     dest0 = np.full(n, pg.NULL_PART, np.int32)
     dest0[::7] = pg.NO_MOVE
-    do, go, ko = O.select(og, cd_o, part, pv, dest0, fr, initial)
-    dg, gg_, kg = pg.select_pass(mem, wg, cd_g, part, pv, dest0, fr, initial)
+    gain0 = np.linspace(-1, 1, n).astype(np.float32)
+    do, go, ko = O.select(og, cd_o, part, pv, dest0, fr, initial, gain=gain0)
+    dg, gg_, kg = pg.select_pass(mem, wg, cd_g, part, pv, dest0, fr, initial, gain=gain0)
+    assert np.array_equal(go[::7], gain0[::7])
     assert ko == kg
     assert np.array_equal(do, dg)
     assert np.array_equal(go.view(np.int32), gg_.view(np.int32))
