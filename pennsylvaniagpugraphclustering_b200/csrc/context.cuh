@@ -4,6 +4,7 @@
 // values the host must read, and a device error flag latched by bounded loops.
 #pragma once
 #include <map>
+#include <mutex>
 #include <vector>
 #include "common.cuh"
 
@@ -176,6 +177,19 @@ struct Context {
         }
     }
 };
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per (kernel, device).
+template <class K>
+inline void set_dynamic_smem_once(K kernel, int bytes, int device) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair((const void*)kernel, device);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return;
+    PGGC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    done[key] = bytes;
+}
 
 // Brackets the launches of one kernel family with CUDA events when profiling.
 struct ProfScope {

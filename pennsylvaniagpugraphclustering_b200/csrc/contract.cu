@@ -338,6 +338,22 @@ __global__ void k_big_place(const i32* list, i64 count, const i64* tstart, const
     }
 }
 
+__global__ void k_max_bound(const i32* list, const i64* d_count, const i64* P, const i64* cstart,
+                            unsigned long long* out) {
+    const i64 count = *d_count;
+    unsigned long long m = 0;
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < count; x += (i64)gridDim.x * blockDim.x) {
+        i32 c = list[x];
+        unsigned long long b = (unsigned long long)(P[cstart[c + 1]] - P[cstart[c]]);
+        m = b > m ? b : m;
+    }
+    for (int d = 16; d >= 1; d >>= 1) {
+        unsigned long long o = __shfl_xor_sync(FULL, m, d);
+        m = o > m ? o : m;
+    }
+    if (lane_id() == 0 && m) atomicMax(out, m);
+}
+
 struct BucketFlag {
     const i64* val;
     i64 lo, hi;  // lo < v <= hi
@@ -370,11 +386,12 @@ struct RowptrOut {
     i64* rp;
     __device__ void operator()(i64 c, i64 excl, i64) const { rp[c] = excl; }
 };
+// unique count of the x-th row of a device-counted list (0 past the count)
 struct ListUIn {
     const i32* list;
     const i64* u;
-    i64 k;
-    __device__ i64 operator()(i64 x) const { return x < k ? u[list[x]] : 0; }
+    const i64* d_count;
+    __device__ i64 operator()(i64 x) const { return x < *d_count ? u[list[x]] : 0; }
 };
 
 template <class W>
@@ -421,8 +438,11 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     scan_apply(ctx, BoundFlag{P.p, cstart.p, 128, HUGE_DEG}, IdxEpiC{lb.p}, nc, nullptr, counts.p + 1);
     scan_apply(ctx, BoundFlag{P.p, cstart.p, HUGE_DEG, (i64)1 << 62}, IdxEpiC{lh.p}, nc, nullptr, counts.p + 2);
     PGGC_CUDA(cudaMemsetAsync(counts.p + 3, 0, sizeof(i64) * 5, ctx.stream));
-    const i64* hc = (const i64*)ctx.readback(counts.p, 3 * sizeof(i64));
-    const i64 n_w = hc[0], n_b = hc[1], n_h = hc[2];
+    k_max_bound<<<64, 256, 0, ctx.stream>>>(lh.p, counts.p + 2, P.p, cstart.p, (unsigned long long*)(counts.p + 7));
+    PGGC_LAUNCH_CHECK();
+    // one round trip: bucket sizes and the largest bound among the huge rows
+    const i64* hc = (const i64*)ctx.readback(counts.p, 8 * sizeof(i64));
+    const i64 n_w = hc[0], n_b = hc[1], n_h = hc[2], max_huge = hc[7];
 
     CArgs<W> a;
     a.g = gv;
@@ -442,16 +462,14 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     }
     if (n_b > 0) {
         size_t sm = (sizeof(V) + sizeof(i32)) * SEL_TS_MAX;
-        PGGC_CUDA(cudaFuncSetAttribute(k_contract_block<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        set_dynamic_smem_once(k_contract_block<W, false>, (int)sm, ctx.device);
         int grid = (int)std::min<i64>(n_b, (i64)ctx.num_sms * 2);
         k_contract_block<W, false><<<grid, 256, sm, ctx.stream>>>(a, lb.p, counts.p + 1, nullptr, nullptr, 0, nc);
         PGGC_LAUNCH_CHECK();
     }
     if (n_h > 0) {
-        // global tables sized for the largest bound (capped by nc)
-        DBuf<i64> mx(ctx, 1);
-        // largest bound among huge rows: bounded by total; use min(maxdeg-sum, nc)
-        i64 maxb = std::min<i64>(total_bound, nc);
+        // global tables sized for the largest bound among the huge rows (capped by nc)
+        i64 maxb = std::min<i64>(max_huge, nc);
         i64 gcap = next_pow2_u32((u32)std::min<i64>(2 * std::max<i64>(maxb, 1), (i64)1 << 30));
         int grid = (int)std::min<i64>(n_h, 16);
         DBuf<i32> gk(ctx, gcap * grid);
@@ -459,20 +477,21 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         k_contract_block<W, true><<<grid, 256, 0, ctx.stream>>>(a, lh.p, counts.p + 2, gk.p, gvv.p, gcap, nc);
         PGGC_LAUNCH_CHECK();
     }
-    // coarse row offsets
+    // coarse row offsets, placement buckets and the big-row total, then one round trip
     scan_apply(ctx, UcountIn{ucount.p, nc}, RowptrOut{cg->rowptr.p}, nc + 1, nullptr, tot.p + 1);
-    i64 nnz_c = ctx.read1(tot.p + 1);
-    ctx.check_device_error();
-    cg->nnz = nnz_c;
-    cg->col = DBuf<i32>(ctx, std::max<i64>(nnz_c, 1));
-    cg->w = DBuf<W>(ctx, std::max<i64>(nnz_c, 1));
-    // placement buckets by unique count
     DBuf<i32> pw(ctx, nc), pb(ctx, nc), ph(ctx, nc);
     scan_apply(ctx, BucketFlag{ucount.p, 0, 32}, IdxEpiC{pw.p}, nc, nullptr, counts.p + 3);
     scan_apply(ctx, BucketFlag{ucount.p, 32, PB_MAX}, IdxEpiC{pb.p}, nc, nullptr, counts.p + 4);
     scan_apply(ctx, BucketFlag{ucount.p, PB_MAX, (i64)1 << 62}, IdxEpiC{ph.p}, nc, nullptr, counts.p + 5);
-    const i64* pc = (const i64*)ctx.readback(counts.p + 3, 3 * sizeof(i64));
-    const i64 p_w = pc[0], p_b = pc[1], p_h = pc[2];
+    DBuf<i64> tstart(ctx, nc + 1);
+    scan_apply(ctx, ListUIn{ph.p, ucount.p, counts.p + 5}, ArrOutExcl{tstart.p}, nc + 1, nullptr, tot.p + 2);
+    PGGC_CUDA(cudaMemcpyAsync(counts.p + 6, tot.p + 1, 2 * sizeof(i64), cudaMemcpyDeviceToDevice, ctx.stream));
+    const i64* pc = (const i64*)ctx.readback(counts.p, 8 * sizeof(i64));
+    const i64 p_w = pc[3], p_b = pc[4], p_h = pc[5], nnz_c = pc[6], tn = pc[7];
+    ctx.check_device_error();
+    cg->nnz = nnz_c;
+    cg->col = DBuf<i32>(ctx, std::max<i64>(nnz_c, 1));
+    cg->w = DBuf<W>(ctx, std::max<i64>(nnz_c, 1));
     if (p_w > 0) {
         int grid = (int)std::min<i64>(ceil_div(p_w, 8), (i64)ctx.num_sms * 8);
         k_place_warp<W><<<grid, 256, 0, ctx.stream>>>(pw.p, counts.p + 3, P.p, cstart.p, ucount.p, cg->rowptr.p, okey.p,
@@ -486,9 +505,6 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         PGGC_LAUNCH_CHECK();
     }
     if (p_h > 0) {
-        DBuf<i64> tstart(ctx, p_h + 1);
-        scan_apply(ctx, ListUIn{ph.p, ucount.p, p_h}, ArrOutExcl{tstart.p}, p_h + 1, nullptr, tot.p + 2);
-        i64 tn = ctx.read1(tot.p + 2);
         DBuf<u64> tk(ctx, tn), tk2(ctx, tn);
         DBuf<V> tv(ctx, tn), tv2(ctx, tn);
         int grid = (int)std::min<i64>(p_h, (i64)ctx.num_sms * 4);

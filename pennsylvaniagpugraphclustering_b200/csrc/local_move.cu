@@ -24,6 +24,7 @@ namespace pggc {
 template <class V>
 struct LMScalars {
     i64 num_cand, split, num_moves, num_new, num_avail, avail_k;
+    unsigned long long new_hint;  // NEW_PART moves counted while compacting the move list
     i64 label_count, best_label_count;
     V uncut, best_uncut, last_pval, pval_sum;
     i64 sumsq_i;
@@ -512,6 +513,20 @@ struct KeepFlag {
     const unsigned char* keep;
     __device__ i64 operator()(i64 x) const { return keep[x]; }
 };
+// move-list compaction that also counts the NEW_PART moves
+struct MoveEpi {
+    const i32* cand;
+    const i32* dest;
+    i32* moves;
+    unsigned long long* new_count;
+    __device__ void operator()(i64 x, i64 excl, i64 v) const {
+        if (v) {
+            i32 i = cand[x];
+            moves[excl] = i;
+            if (dest[i] == NEW_PART) atomicAdd(new_count, 1ull);
+        }
+    }
+};
 struct ListEpi {
     const i32* src;
     i32* dst;
@@ -961,8 +976,7 @@ struct Mover {
             ProfScope ps(ctx, "select_block");
             a.prof = ctx.prof_counter("select_block");
             size_t sm = (sizeof(V) + sizeof(i32)) * SEL_TS_MAX;
-            PGGC_CUDA(cudaFuncSetAttribute(k_select_block<W, CON, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sm));
+            set_dynamic_smem_once(k_select_block<W, CON, false>, (int)sm, ctx.device);
             int grid = (int)std::min<i64>(nb, (i64)ctx.num_sms * 2);
             k_select_block<W, CON, false><<<grid, 256, sm, ctx.stream>>>(a, ord.order1.p + ord.off_large, nb, nullptr,
                                                                          nullptr, 0);
@@ -1017,7 +1031,9 @@ struct Mover {
             k_afterburner_block<W><<<(int)std::min<i64>(nm, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(a);
             PGGC_LAUNCH_CHECK();
         }
-        scan_apply(ctx, KeepFlag{keep.p}, ListEpi{cand.p, moves.p}, n, &sc.p->num_cand, &sc.p->num_moves);
+        PGGC_CUDA(cudaMemsetAsync(&sc.p->new_hint, 0, sizeof(unsigned long long), ctx.stream));
+        scan_apply(ctx, KeepFlag{keep.p}, MoveEpi{cand.p, dest.p, moves.p, &sc.p->new_hint}, n, &sc.p->num_cand,
+                   &sc.p->num_moves);
     }
 
     void set_new_cluster_ids(i64 nmoves_host, i32* constraint) {
@@ -1203,8 +1219,11 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
                 m.afterburner(pm);
                 const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
                 i64 ncand = hs->num_cand, nm = hs->num_moves;
+                const bool any_new = hs->new_hint != 0;
                 if (ncand == 0 || nm == 0) break;
-                if (iter_count > 1 || !is_initial) m.set_new_cluster_ids(nm, constrained ? constraint : nullptr);
+                // set_new_cluster_ids is a no-op without NEW_PART moves (src/local_mover.cpp:236)
+                if ((iter_count > 1 || !is_initial) && any_new)
+                    m.set_new_cluster_ids(nm, constrained ? constraint : nullptr);
                 label_bound = std::min<i64>(label_bound + nm, m.cap);
                 m.perform_moves(nm, best.lambda, label_bound);
                 m.copy_if_improved(best_part, best.total_deg.p, label_bound);
