@@ -120,6 +120,20 @@ pggc_status pggc_cluster_data_set(pggc_context* ctx, pggc_cluster_data* cd, int6
 pggc_status pggc_generate_orderings(pggc_context* ctx, const pggc_graph* g, int32_t* order1, int32_t* order2,
                                     int64_t offsets[4], int mem_kind);
 
+/* Allocation-free generate_orderings.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory -- a host whose framework
+ * owns all device memory through its own pool and budget, or a latency-bound
+ * loop that must stay out of the driver's allocator.  rowptr (n+1), order1, order2 (n) and
+ * offsets (4 int64) are device pointers; work is queued on `stream` (a
+ * cudaStream_t; NULL = legacy default stream) and the call returns without
+ * waiting.  The scratch is a fixed 768 KiB __device__ array inside the library
+ * (held by every GPU that loads it until exit), so n is limited to 16,777,216
+ * (larger n returns PGGC_ERR_INVALID).  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * All calls share the one array: calls whose work overlaps on the GPU race. */
+pggc_status pggc_generate_orderings_noalloc(const int64_t* rowptr, int64_t n, int32_t* order1, int32_t* order2,
+                                            int64_t* offsets, void* stream);
+
 /* ---- local_move_heuristic (src/header/local_mover.h:21-25) ----------------
  * local_move<constrained> (strict = 0) or local_move_strict<constrained>
  * (strict = 1) on partition part_io with cluster_data cd (in/out).

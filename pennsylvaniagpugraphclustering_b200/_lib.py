@@ -69,6 +69,7 @@ _SIGS = {
     "pggc_cluster_data_total_deg": (_ci, [_vp, _vp, _vp, _ci]),
     "pggc_cluster_data_set": (_ci, [_vp, _vp, _i64, _vp, _dbl, _ci]),
     "pggc_generate_orderings": (_ci, [_vp, _vp, _vp, _vp, _vp, _ci]),
+    "pggc_generate_orderings_noalloc": (_ci, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "pggc_local_move": (_ci, [_vp, _vp, _vp, _vp, _ci, _ci, _vp, _i64, _ci, _ci, _ci, _ci, ctypes.POINTER(Stats)]),
     "pggc_select_pass": (_ci, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _flt, _ci, _ci, _vp, _ci, ctypes.POINTER(_i64)]),
     "pggc_build_coarse_graph": (_ci, [_vp, _vp, _vp, _i64, _ci, _PP]),

@@ -251,6 +251,9 @@ struct I64Arr {
 
 }  // namespace
 
+// shared with entry points defined next to their kernels in other files
+void pggc_set_last_error(const char* msg) { g_last_error = msg; }
+
 extern "C" {
 
 const char* pggc_last_error(void) { return g_last_error.c_str(); }

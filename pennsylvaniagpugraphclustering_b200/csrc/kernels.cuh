@@ -5,6 +5,9 @@
 #include <vector>
 #include "scan.cuh"
 
+// sets the thread-local message returned by pggc_last_error()
+void pggc_set_last_error(const char* msg);
+
 namespace pggc {
 
 // Vertices of degree above HUGE_DEG aggregate into global-memory tables; all

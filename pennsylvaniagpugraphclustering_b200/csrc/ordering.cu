@@ -7,7 +7,9 @@
 // per-block bucket counts, one scan turns them into positions, one scatter pass
 // ranks vertices inside each block with warp ballots.  HBM traffic: two reads of
 // the row offsets and one write of each permutation.
+#include <mutex>
 #include "kernels.cuh"
+#include "pggc.h"
 
 namespace pggc {
 
@@ -123,3 +125,118 @@ void generate_orderings(Context& ctx, const i64* rowptr, i64 n, Ordering& o) {
 }
 
 }  // namespace pggc
+
+// ===========================================================================
+// Allocation-free variant of generate_orderings.
+//
+// Some callers cannot allocate device memory at all: a host that hands this
+// library a stream inside an allocator-controlled region (a framework that
+// owns every byte of device memory through its own pool and budget), or a
+// real-time loop that must not touch the driver's allocator.  This entry point serves them: the caller
+// passes the inputs and outputs and a stream, and the only scratch (the
+// per-block bucket counts and the max-degree word) lives in a file-scope
+// __device__ array of fixed size.  That array is part of the module image, so
+// every GPU that loads the library holds it until process exit.
+// ===========================================================================
+namespace pggc {
+
+// Up to NOALLOC_MAX_BLOCKS blocks of 1024 vertices: n <= 16,777,216.
+constexpr i64 NOALLOC_MAX_BLOCKS = 16384;
+constexpr i64 NOALLOC_MAX_N = NOALLOC_MAX_BLOCKS * ORD_THREADS;
+// layout (int64 words): [0, 3B) order1 bucket counts, [3B, 6B) order2 bucket
+// counts (B = NOALLOC_MAX_BLOCKS), then 8 words for the max-degree counter.
+constexpr i64 NOALLOC_WORDS = 6 * NOALLOC_MAX_BLOCKS + 8;
+static __device__ __align__(256) long long g_noalloc_scratch[NOALLOC_WORDS];
+
+// In-place exclusive scan of k int64 values by one 1024-thread block; writes the
+// three bucket starts the reference stores in memory_store::ordering.
+__global__ void __launch_bounds__(1024) k_noalloc_scan(i64* cnt1, i64* cnt2, i64 nb, i64* offsets_out) {
+    __shared__ i64 red[1024 / 32 + 1];
+    for (int which = 0; which < 2; which++) {
+        i64* a = which == 0 ? cnt1 : cnt2;
+        const i64 k = 3 * nb;
+        const i64 per = (k + 1023) / 1024;
+        const i64 lo = (i64)threadIdx.x * per, hi = min(k, lo + per);
+        i64 s = 0;
+        for (i64 i = lo; i < hi; i++) s += a[i];
+        i64 off = block_excl_scan_i64<1024>(s, red, nullptr);
+        for (i64 i = lo; i < hi; i++) {
+            i64 v = a[i];
+            a[i] = off;
+            off += v;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        offsets_out[0] = cnt1[nb];      // offset_large
+        offsets_out[1] = cnt1[2 * nb];  // offset_large2
+        offsets_out[2] = cnt2[nb];      // offset_mid
+        offsets_out[3] = cnt1[2 * nb];  // offset_mid2
+    }
+}
+
+__global__ void k_noalloc_clear(i64* words, int count) {
+    if (threadIdx.x < count) words[threadIdx.x] = 0;
+}
+
+}  // namespace pggc
+
+namespace {
+// device address of g_noalloc_scratch, looked up once per device
+std::mutex g_noalloc_mu;
+long long* g_noalloc_addr[64] = {nullptr};
+}  // namespace
+
+extern "C" pggc_status pggc_generate_orderings_noalloc(const int64_t* rowptr, int64_t n, int32_t* order1,
+                                                       int32_t* order2, int64_t* offsets, void* stream) {
+    using namespace pggc;
+    try {
+        if (n < 0 || n > NOALLOC_MAX_N) {
+            pggc_set_last_error("n exceeds the allocation-free limit of 16,777,216 vertices");
+            return PGGC_ERR_INVALID;
+        }
+        if (!rowptr || !offsets || (n > 0 && (!order1 || !order2))) {
+            pggc_set_last_error("NULL argument");
+            return PGGC_ERR_INVALID;
+        }
+        int dev = 0;
+        PGGC_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) {
+            pggc_set_last_error("device index out of range");
+            return PGGC_ERR_INVALID;
+        }
+        long long* scratch = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(g_noalloc_mu);
+            if (!g_noalloc_addr[dev]) {
+                void* p = nullptr;
+                PGGC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+                g_noalloc_addr[dev] = (long long*)p;
+            }
+            scratch = g_noalloc_addr[dev];
+        }
+        cudaStream_t s = (cudaStream_t)stream;
+        i64* cnt1 = (i64*)scratch;
+        i64* cnt2 = cnt1 + 3 * NOALLOC_MAX_BLOCKS;
+        i64* maxw = cnt1 + 6 * NOALLOC_MAX_BLOCKS;
+        k_noalloc_clear<<<1, 32, 0, s>>>(maxw, 8);
+        PGGC_LAUNCH_CHECK();
+        if (n == 0) {
+            PGGC_CUDA(cudaMemsetAsync(offsets, 0, 4 * sizeof(int64_t), s));
+            return PGGC_OK;
+        }
+        const i64 nb = ceil_div(n, ORD_THREADS);
+        // the counts are fully rewritten by k_order_count; the layout uses the
+        // first 3 * nb words of each half, so the bucket-major strides are nb
+        k_order_count<<<(unsigned)nb, ORD_THREADS, 0, s>>>(rowptr, n, nb, cnt1, cnt2, (unsigned long long*)maxw);
+        PGGC_LAUNCH_CHECK();
+        k_noalloc_scan<<<1, 1024, 0, s>>>(cnt1, cnt2, nb, offsets);
+        PGGC_LAUNCH_CHECK();
+        k_order_scatter<<<(unsigned)nb, ORD_THREADS, 0, s>>>(rowptr, n, nb, cnt1, cnt2, order1, order2);
+        PGGC_LAUNCH_CHECK();
+        return PGGC_OK;
+    } catch (const std::exception& e) {
+        pggc_set_last_error(e.what());
+        return PGGC_ERR_CUDA;
+    }
+}
