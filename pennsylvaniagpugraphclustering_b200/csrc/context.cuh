@@ -10,6 +10,9 @@
 
 namespace pggc {
 
+// workspace slots shared across kernel families (local_move uses 0..31)
+enum WsSlot : int { WS_CONTRACT_GK = 40, WS_CONTRACT_GV = 41, WS_OWN_CLS = 42, WS_OWN_OFF = 43, WS_OWN_CNT = 44 };
+
 // Per-kernel-family timing with CUDA events on the launching stream, plus the
 // algorithmic bytes the kernels report (accumulated on the device per warp and
 // flushed with one atomic per warp).  Off unless enabled.

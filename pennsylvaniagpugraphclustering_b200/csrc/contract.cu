@@ -141,10 +141,9 @@ __device__ __forceinline__ void cchunk(const CArgs<W>& a, i32 c, i64 m0, i64 m1,
     if (leader) ctable_add(keys, vals, mask, u, s, a.err, a.probe_cap);
 }
 
-constexpr int CW_WARPS = 8;
-constexpr int CW_T = 256;
-
-template <class W>
+// warp per coarse row with a per-warp shared-memory table of CW_T slots
+// (rows with bound <= CW_T / 2)
+template <class W, int CW_T, int CW_WARPS>
 __global__ void __launch_bounds__(CW_WARPS * 32) k_contract_warp(CArgs<W> a, const i32* list, const i64* d_count) {
     using V = typename Traits<W>::V;
     __shared__ i32 tk[CW_WARPS][CW_T];
@@ -185,6 +184,8 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_contract_warp(CArgs<W> a, con
     }
 }
 
+// block per coarse row; the table is in shared memory (`gcap` slots, sized to
+// the bucket's largest table) or, with GLOBAL, in a per-block global region
 template <class W, bool GLOBAL>
 __global__ void __launch_bounds__(256) k_contract_block(CArgs<W> a, const i32* list, const i64* d_count, i32* gkeys,
                                                         typename Traits<W>::V* gvals, i64 gcap, i64 nc) {
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(256) k_contract_block(CArgs<W> a, const i32* l
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long wcount;
     V* svals = (V*)smem_raw;
-    i32* skeys = (i32*)(smem_raw + sizeof(V) * SEL_TS_MAX);
+    i32* skeys = (i32*)(smem_raw + sizeof(V) * (GLOBAL ? 0 : gcap));
     const int l = lane_id(), w = threadIdx.x >> 5;
     i32* keys = GLOBAL ? gkeys + (i64)blockIdx.x * gcap : skeys;
     V* vals = GLOBAL ? gvals + (i64)blockIdx.x * gcap : svals;
@@ -259,6 +260,39 @@ __global__ void __launch_bounds__(256) k_place_warp(const i32* list, const i64* 
             col[rowptr[c] + rank] = key;
             wout[rowptr[c] + rank] = to_w<W>(val);
         }
+    }
+}
+
+// 32 < u <= PW_MAX: the warp stages the row in shared memory and each lane
+// ranks its entries against all of them
+constexpr int PW_MAX = 256;
+constexpr int PW_WARPS = 8;
+
+template <class W>
+__global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* list, const i64* d_count, const i64* P,
+                                                                   const i64* cstart, const i64* ucount,
+                                                                   const i64* rowptr, const i32* skey,
+                                                                   const typename Traits<W>::V* sval, i32* col,
+                                                                   W* wout) {
+    __shared__ i32 kk[PW_WARPS][PW_MAX];
+    const int l = lane_id(), w = threadIdx.x >> 5;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    const i64 count = *d_count;
+    for (i64 x = gw; x < count; x += nw) {
+        i32 c = list[x];
+        i64 src = P[cstart[c]];
+        int u = (int)ucount[c];
+        for (int s = l; s < u; s += 32) kk[w][s] = skey[src + s];
+        __syncwarp();
+        for (int s = l; s < u; s += 32) {
+            i32 key = kk[w][s];
+            int rank = 0;
+            for (int t = 0; t < u; t++) rank += kk[w][t] < key ? 1 : 0;
+            col[rowptr[c] + rank] = key;
+            wout[rowptr[c] + rank] = to_w<W>(sval[src + s]);
+        }
+        __syncwarp();
     }
 }
 
@@ -362,13 +396,19 @@ struct BucketFlag {
         return (v > lo && v <= hi) ? 1 : 0;
     }
 };
+// lo < bound <= hi, and for mode 1 / 2 also U = min(bound, nc) <= / > 4096
 struct BoundFlag {
     const i64* P;
     const i64* cstart;
-    i64 lo, hi;
+    i64 lo, hi, nc;
+    int mode;
     __device__ i64 operator()(i64 c) const {
         i64 v = P[cstart[c + 1]] - P[cstart[c]];
-        return (v > lo && v <= hi) ? 1 : 0;
+        if (!(v > lo && v <= hi)) return 0;
+        i64 U = v < nc ? v : nc;
+        if (mode == 1) return U <= HUGE_DEG ? 1 : 0;
+        if (mode == 2) return U > HUGE_DEG ? 1 : 0;
+        return 1;
     }
 };
 struct IdxEpiC {
@@ -431,18 +471,23 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     DBuf<i32> okey(ctx, std::max<i64>(total_bound, 1));
     DBuf<V> oval(ctx, std::max<i64>(total_bound, 1));
 
-    // bucket lists by bound
-    DBuf<i32> lw(ctx, nc), lb(ctx, nc), lh(ctx, nc);
-    DBuf<i64> counts(ctx, 8);
-    scan_apply(ctx, BoundFlag{P.p, cstart.p, -1, 128}, IdxEpiC{lw.p}, nc, nullptr, counts.p + 0);
-    scan_apply(ctx, BoundFlag{P.p, cstart.p, 128, HUGE_DEG}, IdxEpiC{lb.p}, nc, nullptr, counts.p + 1);
-    scan_apply(ctx, BoundFlag{P.p, cstart.p, HUGE_DEG, (i64)1 << 62}, IdxEpiC{lh.p}, nc, nullptr, counts.p + 2);
-    PGGC_CUDA(cudaMemsetAsync(counts.p + 3, 0, sizeof(i64) * 5, ctx.stream));
+    // bucket lists by table size U = min(bound, nc) and bound:
+    //   small warp rows (bound <= 32), medium warp rows (bound <= 256),
+    //   block rows with a shared-memory table (U <= 4096), global-table rows
+    DBuf<i32> lw(ctx, nc), lm(ctx, nc), lb(ctx, nc), lh(ctx, nc);
+    DBuf<i64> counts(ctx, 12);
+    PGGC_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(i64) * 12, ctx.stream));
+    scan_apply(ctx, BoundFlag{P.p, cstart.p, -1, 32, nc, 0}, IdxEpiC{lw.p}, nc, nullptr, counts.p + 0);
+    scan_apply(ctx, BoundFlag{P.p, cstart.p, 32, 256, nc, 0}, IdxEpiC{lm.p}, nc, nullptr, counts.p + 8);
+    scan_apply(ctx, BoundFlag{P.p, cstart.p, 256, (i64)1 << 62, nc, 1}, IdxEpiC{lb.p}, nc, nullptr, counts.p + 1);
+    scan_apply(ctx, BoundFlag{P.p, cstart.p, 256, (i64)1 << 62, nc, 2}, IdxEpiC{lh.p}, nc, nullptr, counts.p + 2);
     k_max_bound<<<64, 256, 0, ctx.stream>>>(lh.p, counts.p + 2, P.p, cstart.p, (unsigned long long*)(counts.p + 7));
     PGGC_LAUNCH_CHECK();
-    // one round trip: bucket sizes and the largest bound among the huge rows
-    const i64* hc = (const i64*)ctx.readback(counts.p, 8 * sizeof(i64));
-    const i64 n_w = hc[0], n_b = hc[1], n_h = hc[2], max_huge = hc[7];
+    k_max_bound<<<64, 256, 0, ctx.stream>>>(lb.p, counts.p + 1, P.p, cstart.p, (unsigned long long*)(counts.p + 9));
+    PGGC_LAUNCH_CHECK();
+    // one round trip: bucket sizes and the largest bounds
+    const i64* hc = (const i64*)ctx.readback(counts.p, 12 * sizeof(i64));
+    const i64 n_w = hc[0], n_b = hc[1], n_h = hc[2], max_huge = hc[7], n_m = hc[8], max_block = hc[9];
 
     CArgs<W> a;
     a.g = gv;
@@ -456,38 +501,52 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     a.err = ctx.d_err;
     a.probe_cap = ctx.probe_cap;
     if (n_w > 0) {
-        int grid = (int)std::min<i64>(ceil_div(n_w, CW_WARPS), (i64)ctx.num_sms * 8);
-        k_contract_warp<W><<<grid, CW_WARPS * 32, 0, ctx.stream>>>(a, lw.p, counts.p + 0);
+        constexpr int WARPS = 8;
+        int grid = (int)std::min<i64>(ceil_div(n_w, WARPS), (i64)ctx.num_sms * 16);
+        k_contract_warp<W, 64, WARPS><<<grid, WARPS * 32, 0, ctx.stream>>>(a, lw.p, counts.p + 0);
+        PGGC_LAUNCH_CHECK();
+    }
+    if (n_m > 0) {
+        constexpr int WARPS = 4;
+        int grid = (int)std::min<i64>(ceil_div(n_m, WARPS), (i64)ctx.num_sms * 16);
+        k_contract_warp<W, 512, WARPS><<<grid, WARPS * 32, 0, ctx.stream>>>(a, lm.p, counts.p + 8);
         PGGC_LAUNCH_CHECK();
     }
     if (n_b > 0) {
-        size_t sm = (sizeof(V) + sizeof(i32)) * SEL_TS_MAX;
-        set_dynamic_smem_once(k_contract_block<W, false>, (int)sm, ctx.device);
-        int grid = (int)std::min<i64>(n_b, (i64)ctx.num_sms * 2);
-        k_contract_block<W, false><<<grid, 256, sm, ctx.stream>>>(a, lb.p, counts.p + 1, nullptr, nullptr, 0, nc);
+        // table sized to the largest row of the bucket
+        i64 tmax = next_pow2_u32((u32)(2 * std::max<i64>(std::min<i64>(max_block, nc), 1)));
+        size_t sm = (sizeof(V) + sizeof(i32)) * (size_t)tmax;
+        set_dynamic_smem_once(k_contract_block<W, false>, (int)((sizeof(V) + sizeof(i32)) * SEL_TS_MAX), ctx.device);
+        int per_sm = 0;
+        PGGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_block<W, false>, 256, sm));
+        int grid = (int)std::min<i64>(n_b, (i64)ctx.num_sms * std::max(per_sm, 1));
+        k_contract_block<W, false><<<grid, 256, sm, ctx.stream>>>(a, lb.p, counts.p + 1, nullptr, nullptr, tmax, nc);
         PGGC_LAUNCH_CHECK();
     }
     if (n_h > 0) {
-        // global tables sized for the largest bound among the huge rows (capped by nc)
+        // global tables sized for the largest table among the huge rows, one
+        // region per resident block, at most 2 GiB of tables
         i64 maxb = std::min<i64>(max_huge, nc);
         i64 gcap = next_pow2_u32((u32)std::min<i64>(2 * std::max<i64>(maxb, 1), (i64)1 << 30));
-        int grid = (int)std::min<i64>(n_h, 16);
-        DBuf<i32> gk(ctx, gcap * grid);
-        DBuf<V> gvv(ctx, gcap * grid);
-        k_contract_block<W, true><<<grid, 256, 0, ctx.stream>>>(a, lh.p, counts.p + 2, gk.p, gvv.p, gcap, nc);
+        i64 by_mem = std::max<i64>(1, ((i64)2 << 30) / (gcap * (i64)(sizeof(V) + sizeof(i32))));
+        int grid = (int)std::min<i64>(std::min<i64>(n_h, (i64)ctx.num_sms * 2), by_mem);
+        i32* gk = ctx.ws_get<i32>(WS_CONTRACT_GK, gcap * grid);
+        V* gvv = ctx.ws_get<V>(WS_CONTRACT_GV, gcap * grid);
+        k_contract_block<W, true><<<grid, 256, 0, ctx.stream>>>(a, lh.p, counts.p + 2, gk, gvv, gcap, nc);
         PGGC_LAUNCH_CHECK();
     }
     // coarse row offsets, placement buckets and the big-row total, then one round trip
     scan_apply(ctx, UcountIn{ucount.p, nc}, RowptrOut{cg->rowptr.p}, nc + 1, nullptr, tot.p + 1);
-    DBuf<i32> pw(ctx, nc), pb(ctx, nc), ph(ctx, nc);
+    DBuf<i32> pw(ctx, nc), pr(ctx, nc), pb(ctx, nc), ph(ctx, nc);
     scan_apply(ctx, BucketFlag{ucount.p, 0, 32}, IdxEpiC{pw.p}, nc, nullptr, counts.p + 3);
-    scan_apply(ctx, BucketFlag{ucount.p, 32, PB_MAX}, IdxEpiC{pb.p}, nc, nullptr, counts.p + 4);
+    scan_apply(ctx, BucketFlag{ucount.p, 32, PW_MAX}, IdxEpiC{pr.p}, nc, nullptr, counts.p + 10);
+    scan_apply(ctx, BucketFlag{ucount.p, PW_MAX, PB_MAX}, IdxEpiC{pb.p}, nc, nullptr, counts.p + 4);
     scan_apply(ctx, BucketFlag{ucount.p, PB_MAX, (i64)1 << 62}, IdxEpiC{ph.p}, nc, nullptr, counts.p + 5);
     DBuf<i64> tstart(ctx, nc + 1);
     scan_apply(ctx, ListUIn{ph.p, ucount.p, counts.p + 5}, ArrOutExcl{tstart.p}, nc + 1, nullptr, tot.p + 2);
     PGGC_CUDA(cudaMemcpyAsync(counts.p + 6, tot.p + 1, 2 * sizeof(i64), cudaMemcpyDeviceToDevice, ctx.stream));
-    const i64* pc = (const i64*)ctx.readback(counts.p, 8 * sizeof(i64));
-    const i64 p_w = pc[3], p_b = pc[4], p_h = pc[5], nnz_c = pc[6], tn = pc[7];
+    const i64* pc = (const i64*)ctx.readback(counts.p, 12 * sizeof(i64));
+    const i64 p_w = pc[3], p_b = pc[4], p_h = pc[5], nnz_c = pc[6], tn = pc[7], p_r = pc[10];
     ctx.check_device_error();
     cg->nnz = nnz_c;
     cg->col = DBuf<i32>(ctx, std::max<i64>(nnz_c, 1));
@@ -496,6 +555,13 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         int grid = (int)std::min<i64>(ceil_div(p_w, 8), (i64)ctx.num_sms * 8);
         k_place_warp<W><<<grid, 256, 0, ctx.stream>>>(pw.p, counts.p + 3, P.p, cstart.p, ucount.p, cg->rowptr.p, okey.p,
                                                       oval.p, cg->col.p, cg->w.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    if (p_r > 0) {
+        int grid = (int)std::min<i64>(ceil_div(p_r, PW_WARPS), (i64)ctx.num_sms * 8);
+        k_place_warp_rank<W><<<grid, PW_WARPS * 32, 0, ctx.stream>>>(pr.p, counts.p + 10, P.p, cstart.p, ucount.p,
+                                                                     cg->rowptr.p, okey.p, oval.p, cg->col.p,
+                                                                     cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
     if (p_b > 0) {
