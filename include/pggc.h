@@ -184,6 +184,43 @@ pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_clu
 pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, int objective,
                                   double lambda_mult, int mem_kind, double* objective_out, double* raw_obj_out);
 
+/* ---- learned move filter (no counterpart in the reference) ----------------
+ * A network that decides which vertices a local-move sweep evaluates; the
+ * gains of the evaluated vertices stay exact.  8 features per vertex ->
+ * 32 -> 32 (ReLU) -> 1 logit, BF16 weights and FP32 accumulation.  Parameters
+ * are PGGC_MLP_PARAMS FP32 values: W1[32][8] | b1[32] | W2[32][32] | b2[32] |
+ * W3[32] | b3 (weights [out][in]).  Features are rows of PGGC_MLP_FEATURES
+ * floats; labels are 0/1 floats (1 = the vertex moved). */
+#define PGGC_MLP_PARAMS 1377
+#define PGGC_MLP_FEATURES 8
+
+/* logits of `count` feature rows (tensor-core inference path) */
+pggc_status pggc_mlp_infer(pggc_context* ctx, const float* params, const float* features, int64_t count, int mem_kind,
+                           float* logits_out);
+/* mean positive-weighted binary cross-entropy of the rows and its gradient
+ * (PGGC_MLP_PARAMS floats); count <= 1,048,576 */
+pggc_status pggc_mlp_loss_grad(pggc_context* ctx, const float* params, const float* features, const float* labels,
+                               int64_t count, float pos_weight, int mem_kind, float* grad_out, float* loss_out);
+/* Adam on shuffled mini-batches of `batch` rows for `epochs` epochs; params_io
+ * is updated in place; epoch_loss_out (host, `epochs` floats, may be NULL)
+ * receives each epoch's mean batch loss */
+pggc_status pggc_mlp_train(pggc_context* ctx, float* params_io, const float* features, const float* labels,
+                           int64_t count, int mem_kind, int epochs, int batch, float lr, float pos_weight,
+                           uint64_t seed, float* epoch_loss_out);
+/* start logging (features, label) samples from the context's plain sweeps:
+ * each evaluated vertex is sampled with probability sample_rate, up to
+ * `capacity` rows */
+pggc_status pggc_filter_log_start(pggc_context* ctx, int64_t capacity, double sample_rate, uint64_t seed);
+/* stop logging and copy out min(rows, capacity) rows; *count_out = rows logged */
+pggc_status pggc_filter_log_stop(pggc_context* ctx, float* features_out, float* labels_out, int64_t capacity,
+                                 int mem_kind, int64_t* count_out);
+/* filter the context's sweeps with this network (host params): vertices whose
+ * logit is below threshold_logit are not evaluated.  params NULL disables it.
+ * The finest level's last local move of each pass always runs unfiltered. */
+pggc_status pggc_filter_enable(pggc_context* ctx, const float* params, float threshold_logit);
+/* vertices evaluated / skipped by the filter since the last reset */
+pggc_status pggc_filter_stats(pggc_context* ctx, int64_t* evaluated, int64_t* skipped, int reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,13 @@ _SIGS = {
     "pggc_cluster_data_set": (_ci, [_vp, _vp, _i64, _vp, _dbl, _ci]),
     "pggc_generate_orderings": (_ci, [_vp, _vp, _vp, _vp, _vp, _ci]),
     "pggc_generate_orderings_noalloc": (_ci, [_vp, _i64, _vp, _vp, _vp, _vp]),
+    "pggc_mlp_infer": (_ci, [_vp, _vp, _vp, _i64, _ci, _vp]),
+    "pggc_mlp_loss_grad": (_ci, [_vp, _vp, _vp, _vp, _i64, _flt, _ci, _vp, _vp]),
+    "pggc_mlp_train": (_ci, [_vp, _vp, _vp, _vp, _i64, _ci, _ci, _ci, _flt, _flt, _u64, _vp]),
+    "pggc_filter_log_start": (_ci, [_vp, _i64, _dbl, _u64]),
+    "pggc_filter_log_stop": (_ci, [_vp, _vp, _vp, _i64, _ci, ctypes.POINTER(_i64)]),
+    "pggc_filter_enable": (_ci, [_vp, _vp, _flt]),
+    "pggc_filter_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _ci]),
     "pggc_local_move": (_ci, [_vp, _vp, _vp, _vp, _ci, _ci, _vp, _i64, _ci, _ci, _ci, _ci, ctypes.POINTER(Stats)]),
     "pggc_select_pass": (_ci, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _flt, _ci, _ci, _vp, _ci, ctypes.POINTER(_i64)]),
     "pggc_build_coarse_graph": (_ci, [_vp, _vp, _vp, _i64, _ci, _PP]),

@@ -2,6 +2,7 @@
 #include <cstring>
 #include <string>
 #include "kernels.cuh"
+#include "mlp_train.cuh"
 #include "pggc.h"
 
 using namespace pggc;
@@ -762,6 +763,158 @@ pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const 
             if (objective_out) *objective_out = cs.get_objective();
             if (raw_obj_out) *raw_obj_out = cs.obj;
         });
+    });
+}
+
+// ---- learned move filter ---------------------------------------------------
+static void filter_free_log(Context& c) {
+    auto& F = c.filt;
+    for (void* q : {(void*)F.log_x, (void*)F.log_y, (void*)F.log_v, (void*)F.log_cnt})
+        if (q) PGGC_CUDA(cudaFreeAsync(q, c.stream));
+    F.log_x = F.log_y = nullptr;
+    F.log_v = nullptr;
+    F.log_cnt = nullptr;
+    F.log_cap = 0;
+}
+
+pggc_status pggc_mlp_infer(pggc_context* ctx, const float* params, const float* features, int64_t count, int mem_kind,
+                           float* logits_out) {
+    return guarded([&] {
+        need(ctx && params && (count == 0 || (features && logits_out)), "NULL argument");
+        need(count >= 0, "count must be >= 0");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        In<float> p(c, params, MLP_PARAMS, mem_kind);
+        In<float> x(c, features, count * MLP_IN, mem_kind);
+        Out<float> out(c, logits_out, count, mem_kind, false);
+        DBuf<MlpDev> net(c, 1);
+        mlp_pack(c, p.p, net.p);
+        mlp_infer(c, net.p, x.p, count, out.p);
+        out.finish();
+        c.sync();
+    });
+}
+
+pggc_status pggc_mlp_loss_grad(pggc_context* ctx, const float* params, const float* features, const float* labels,
+                               int64_t count, float pos_weight, int mem_kind, float* grad_out, float* loss_out) {
+    return guarded([&] {
+        need(ctx && params && features && labels && grad_out && loss_out, "NULL argument");
+        need(count > 0 && count <= (1 << 20), "count must be in [1, 1048576]");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        In<float> p(c, params, MLP_PARAMS, mem_kind);
+        In<float> x(c, features, count * MLP_IN, mem_kind);
+        In<float> y(c, labels, count, mem_kind);
+        Out<float> g(c, grad_out, MLP_PARAMS, mem_kind, false);
+        Out<float> l(c, loss_out, 1, mem_kind, false);
+        mlp_loss_grad(c, p.p, x.p, y.p, nullptr, 0, (int)count, pos_weight, g.p, l.p);
+        g.finish();
+        l.finish();
+        c.sync();
+    });
+}
+
+pggc_status pggc_mlp_train(pggc_context* ctx, float* params_io, const float* features, const float* labels,
+                           int64_t count, int mem_kind, int epochs, int batch, float lr, float pos_weight,
+                           uint64_t seed, float* epoch_loss_out) {
+    return guarded([&] {
+        need(ctx && params_io && features && labels, "NULL argument");
+        need(count > 0 && epochs >= 0 && batch > 0 && batch <= (1 << 20), "invalid training sizes");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        Out<float> p(c, params_io, MLP_PARAMS, mem_kind, true);
+        In<float> x(c, features, count * MLP_IN, mem_kind);
+        In<float> y(c, labels, count, mem_kind);
+        std::vector<float> losses;
+        mlp_train(c, p.p, x.p, y.p, count, epochs, batch, lr, pos_weight, seed, epoch_loss_out ? &losses : nullptr);
+        p.finish();
+        c.sync();
+        if (epoch_loss_out)
+            for (size_t i = 0; i < losses.size(); i++) epoch_loss_out[i] = losses[i];
+    });
+}
+
+pggc_status pggc_filter_log_start(pggc_context* ctx, int64_t capacity, double sample_rate, uint64_t seed) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL argument");
+        need(capacity > 0 && sample_rate > 0.0 && sample_rate <= 1.0, "capacity must be > 0, sample_rate in (0, 1]");
+        Context& c = *ctx->ctx;
+        need(c.filt.mode != 2, "the filter is enabled; disable it before logging");
+        filter_free_log(c);
+        auto& F = c.filt;
+        F.log_x = c.alloc<float>(capacity * MLP_IN);
+        F.log_y = c.alloc<float>(capacity);
+        F.log_v = c.alloc<i32>(capacity);
+        F.log_cnt = c.alloc<unsigned long long>(2);
+        PGGC_CUDA(cudaMemsetAsync(F.log_cnt, 0, 2 * sizeof(unsigned long long), c.stream));
+        F.log_cap = capacity;
+        const double r = sample_rate * 4294967296.0;
+        F.log_rate = r >= 4294967295.0 ? 0xFFFFFFFFu : (u32)r;
+        F.log_seed = seed;
+        F.mode = 1;
+        c.sync();
+    });
+}
+
+pggc_status pggc_filter_log_stop(pggc_context* ctx, float* features_out, float* labels_out, int64_t capacity,
+                                 int mem_kind, int64_t* count_out) {
+    return guarded([&] {
+        need(ctx && count_out, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        auto& F = c.filt;
+        need(F.mode == 1 && F.log_cnt, "logging is not active");
+        const i64 rows = std::min<i64>((i64)c.read1(F.log_cnt), F.log_cap);
+        const i64 k = std::min<i64>(rows, std::max<i64>(capacity, 0));
+        auto kind = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (k > 0 && features_out)
+            PGGC_CUDA(cudaMemcpyAsync(features_out, F.log_x, sizeof(float) * k * MLP_IN, kind, c.stream));
+        if (k > 0 && labels_out) PGGC_CUDA(cudaMemcpyAsync(labels_out, F.log_y, sizeof(float) * k, kind, c.stream));
+        c.sync();
+        *count_out = rows;
+        filter_free_log(c);
+        F.mode = 0;
+        c.sync();
+    });
+}
+
+pggc_status pggc_filter_enable(pggc_context* ctx, const float* params, float threshold_logit) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL argument");
+        Context& c = *ctx->ctx;
+        auto& F = c.filt;
+        need(F.mode != 1, "logging is active; stop it before enabling the filter");
+        if (!params) {
+            F.mode = 0;
+            return;
+        }
+        if (!F.params) F.params = c.alloc<float>(MLP_PARAMS);
+        if (!F.net) F.net = c.alloc<MlpDev>(1);
+        if (!F.stats) {
+            F.stats = c.alloc<unsigned long long>(2);
+            PGGC_CUDA(cudaMemsetAsync(F.stats, 0, 2 * sizeof(unsigned long long), c.stream));
+        }
+        PGGC_CUDA(cudaMemcpyAsync(F.params, params, sizeof(float) * MLP_PARAMS, cudaMemcpyHostToDevice, c.stream));
+        mlp_pack(c, F.params, F.net);
+        F.threshold = threshold_logit;
+        F.mode = 2;
+        c.sync();
+    });
+}
+
+pggc_status pggc_filter_stats(pggc_context* ctx, int64_t* evaluated, int64_t* skipped, int reset) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL argument");
+        Context& c = *ctx->ctx;
+        auto& F = c.filt;
+        unsigned long long h[2] = {0, 0};
+        if (F.stats) {
+            PGGC_CUDA(cudaMemcpyAsync(h, F.stats, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+            c.sync();
+            if (reset) PGGC_CUDA(cudaMemsetAsync(F.stats, 0, sizeof(h), c.stream));
+        }
+        if (evaluated) *evaluated = (int64_t)h[0];
+        if (skipped) *skipped = (int64_t)h[1];
     });
 }
 

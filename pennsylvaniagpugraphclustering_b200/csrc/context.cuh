@@ -6,12 +6,16 @@
 #include <map>
 #include <mutex>
 #include <vector>
+#include <nvtx3/nvToolsExt.h>
 #include "common.cuh"
 
 namespace pggc {
 
+struct MlpDev;
+
 // workspace slots shared across kernel families (local_move uses 0..31)
-enum WsSlot : int { WS_CONTRACT_GK = 40, WS_CONTRACT_GV = 41, WS_OWN_CLS = 42, WS_OWN_OFF = 43, WS_OWN_CNT = 44 };
+enum WsSlot : int { WS_CONTRACT_GK = 40, WS_CONTRACT_GV = 41, WS_OWN_CLS = 42, WS_OWN_OFF = 43, WS_OWN_CNT = 44,
+                    WS_MLP_SCRATCH = 45 };
 
 // Per-kernel-family timing with CUDA events on the launching stream, plus the
 // algorithmic bytes the kernels report (accumulated on the device per warp and
@@ -39,6 +43,25 @@ struct Context {
     std::map<std::string, ProfStat> prof;
     std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
     std::vector<cudaEvent_t> ev_pool;
+    // learned move filter (filter.cuh): mode 0 off, 1 log (features, label)
+    // samples from plain sweeps, 2 skip the vertices the network rejects
+    struct Filter {
+        int mode = 0;
+        MlpDev* net = nullptr;                  // BF16 inference copy (device)
+        float* params = nullptr;                // FP32 master copy (device)
+        float threshold = 0.f;                  // logit below which a vertex is skipped
+        bool suspended = false;                 // set by the driver around exact sweeps
+        float* log_x = nullptr;                 // [log_cap][8]
+        float* log_y = nullptr;                 // [log_cap]
+        i32* log_v = nullptr;                   // [log_cap]
+        unsigned long long* log_cnt = nullptr;  // [0] rows written, [1] first row of the current sweep
+        i64 log_cap = 0;
+        u32 log_rate = 0;                       // a row is sampled when its hash is below this
+        u64 log_seed = 0;
+        unsigned long long* stats = nullptr;    // [0] vertices evaluated, [1] skipped
+        int level = 0;                          // current level, set by the multilevel driver
+        i32 stamp = 0;                          // sweep counter (moved-last-sweep feature)
+    } filt;
 
     explicit Context(int dev) : device(dev) {
         PGGC_CUDA(cudaSetDevice(dev));
@@ -84,6 +107,9 @@ struct Context {
             cudaEventDestroy(pe.second.second);
         }
         for (auto e : ev_pool) cudaEventDestroy(e);
+        for (void* q : {(void*)filt.net, (void*)filt.params, (void*)filt.log_x, (void*)filt.log_y, (void*)filt.log_v,
+                        (void*)filt.log_cnt, (void*)filt.stats})
+            if (q) cudaFreeAsync(q, stream);
         if (d_prof) cudaFreeAsync(d_prof, stream);
         if (d_err) cudaFreeAsync(d_err, stream);
         if (stream) cudaStreamSynchronize(stream);
@@ -141,6 +167,10 @@ struct Context {
         PGGC_CUDA(cudaEventCreate(&e));
         return e;
     }
+    // algorithmic bytes known on the host (sizes of the arrays a family streams)
+    void prof_add_bytes(const std::string& family, double bytes) {
+        if (profiling) prof[family].bytes += bytes;
+    }
     void prof_record(const std::string& family, cudaEvent_t a, cudaEvent_t b) {
         prof_pending.push_back({family, {a, b}});
         if (prof_pending.size() >= 8192) prof_flush();
@@ -194,12 +224,15 @@ inline void set_dynamic_smem_once(K kernel, int bytes, int device) {
     done[key] = bytes;
 }
 
-// Brackets the launches of one kernel family with CUDA events when profiling.
+// Brackets the launches of one kernel family with CUDA events when profiling,
+// and always with an NVTX push/pop range of the family's name (free unless a
+// tool such as ncu --nvtx is attached; lets a capture select one family).
 struct ProfScope {
     Context& ctx;
     const char* family;
     cudaEvent_t a = nullptr, b = nullptr;
     ProfScope(Context& c, const char* f) : ctx(c), family(f) {
+        nvtxRangePushA(f);
         if (ctx.profiling) {
             a = ctx.take_event();
             PGGC_CUDA(cudaEventRecord(a, ctx.stream));
@@ -210,6 +243,7 @@ struct ProfScope {
             b = ctx.take_event();
             if (cudaEventRecord(b, ctx.stream) == cudaSuccess) ctx.prof_record(family, a, b);
         }
+        nvtxRangePop();
     }
 };
 

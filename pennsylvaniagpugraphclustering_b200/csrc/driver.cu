@@ -138,8 +138,9 @@ void make_cluster_state(Context& ctx, const Graph<W>& g, int kind, double mult, 
             return ctx.read1(sd.p);
         }
     };
+    cs.vol_total = sum_vw();
     if (kind == OBJ_MOD || kind == OBJ_WMOD) {
-        double gdeg = g.uniform ? (double)g.nnz : sum_vw();
+        double gdeg = g.uniform ? (double)g.nnz : cs.vol_total;
         cs.inv_gdeg = 1.0 / gdeg;
         cs.lambda = mult * cs.inv_gdeg;
     } else if (kind == OBJ_CPM) {
@@ -211,6 +212,7 @@ void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits
         double old_obj = rfd.obj;
         bool init = !improve && levels.size() == 1;
         generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        ctx.filt.level = (int)levels.size() - 1;
         local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, true, false, -1, &ms);
         if (c.nnz > 100000 && old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, false, -1, &ms);
         if (old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, true, -1, &ms);
@@ -249,7 +251,12 @@ void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits
         PGGC_LAUNCH_CHECK();
         if (plus) {
             generate_orderings(ctx, c.view().rowptr, c.n, ord);
+            // the finest level's last local move runs unfiltered: the exact
+            // sweeps that catch what the learned filter skipped
+            ctx.filt.level = (int)i;
+            ctx.filt.suspended = i == 0;
             local_move<W>(ctx, c, ord, parts[i].p, rfd, false, false, nullptr, true, false, -1, &ms);
+            ctx.filt.suspended = false;
         }
     }
     copy_d2d(ctx, labels_out, parts[0].p, n);
@@ -290,6 +297,7 @@ void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Trait
         DBuf<i32> part(ctx, std::max<i64>(c.n, 1));
         iota<i32>(ctx, part.p, c.n);
         generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        ctx.filt.level = (int)levels.size() - 1;
         local_move<W>(ctx, c, ord, part.p, rfd, true, constrained, constrained ? constraint.p : nullptr, true, false, -1,
                       &ms);
         if (constrained && rfd.label_count == c.n)
@@ -332,7 +340,10 @@ void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Trait
         k_project<<<vgrid(ctx, c.n), 256, 0, ctx.stream>>>(c.n, parts[i].p, parts[i + 1].p);
         PGGC_LAUNCH_CHECK();
         generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        ctx.filt.level = (int)i;
+        ctx.filt.suspended = i == 0;
         local_move<W>(ctx, c, ord, parts[i].p, rfd, false, false, nullptr, true, false, -1, &ms);
+        ctx.filt.suspended = false;
     }
     copy_d2d(ctx, labels_out, parts[0].p, top.n);
     if (st) {

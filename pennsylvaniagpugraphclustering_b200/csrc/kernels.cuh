@@ -71,6 +71,7 @@ struct ClusterState {
     double lambda = 1.0;
     int kind = OBJ_LCC;
     double inv_gdeg = 0.0, v_total = 0.0, g_deg = 0.0;
+    double vol_total = 0.0;  // sum of vertex weights (features of the learned filter)
     double get_objective() const {
         switch (kind) {
             case OBJ_MOD:

@@ -563,6 +563,11 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     PGGC_LAUNCH_CHECK();
     i64 nc = ctx.read1(tot.p);
     ctx.check_device_error();
+    // algorithmic bytes: two adjacency passes (pick, inner connectivity) each
+    // reading column, weight, constraint and label of the neighbour; about ten
+    // n-sized int32 passes (orderings, sort keys, trees, breaks, relabel)
+    ctx.prof_add_bytes("leiden_refine", (double)g.nnz * 2.0 * (4.0 + (g.uniform ? 0.0 : sizeof(W)) + 4.0 + 4.0) +
+                                            (double)n * 10.0 * 4.0);
     return nc;
 }
 

@@ -18,6 +18,7 @@
 //  * One host round trip per sweep (candidate and move counts); everything else
 //    reads counts from device memory.
 #include "kernels.cuh"
+#include "filter.cuh"
 
 namespace pggc {
 
@@ -49,6 +50,37 @@ __device__ __forceinline__ void warp_best(Best& b) {
         float oj = __shfl_xor_sync(FULL, b.jc, d);
         i32 oc = __shfl_xor_sync(FULL, b.c, d);
         if (better(oj, oc, b)) b = Best{oj, oc};
+    }
+}
+
+// A slice of a vertex list whose bounds live on the host or in device memory.
+struct Range {
+    const i32* list;
+    const i64* d_lo;
+    const i64* d_hi;
+    i64 lo, hi;
+    __device__ __forceinline__ i64 begin() const { return d_lo ? *d_lo : lo; }
+    __device__ __forceinline__ i64 end() const { return d_hi ? *d_hi : hi; }
+};
+inline Range host_range(const i32* list, i64 lo, i64 hi) { return Range{list, nullptr, nullptr, lo, hi}; }
+inline Range dev_range(const i32* list, const i64* d_lo, const i64* d_hi) { return Range{list, d_lo, d_hi, 0, 0}; }
+
+// canonical per-vertex sum by a G-lane group (exact match of the 32-lane
+// association for degree <= 2G; integer sums are order-free)
+template <int G, class V, class F>
+__device__ __forceinline__ V group_vsum(i64 b, i64 e, int r, F term) {
+    if constexpr (std::is_same<V, double>::value) {
+        double acc = 0.0;
+        for (i64 j = b + r; j < e; j += G) acc += term(j);
+#pragma unroll
+        for (int d = G / 2; d >= 1; d >>= 1) acc = acc + __shfl_xor_sync(FULL, acc, d);
+        return acc;
+    } else {
+        i64 acc = 0;
+        for (i64 j = b + r; j < e; j += G) acc += term(j);
+#pragma unroll
+        for (int d = G / 2; d >= 1; d >>= 1) acc += __shfl_xor_sync(FULL, acc, d);
+        return acc;
     }
 }
 
@@ -192,16 +224,17 @@ constexpr int SELW_WARPS = 8;
 constexpr int SELW_T = 256;
 
 template <class W, bool CON>
-__global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, const i32* list, i64 count) {
+__global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, Range rg) {
     using V = typename Traits<W>::V;
     __shared__ i32 tk[SELW_WARPS][SELW_T];
     __shared__ V tv[SELW_WARPS][SELW_T];
     const int l = lane_id(), w = threadIdx.x >> 5;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    const i64 lo = rg.begin(), count = rg.end();
     unsigned long long pb = 0;
-    for (i64 x = gw; x < count; x += nw) {
-        i32 i = list[x];
+    for (i64 x = lo + gw; x < count; x += nw) {
+        i32 i = rg.list[x];
         if (a.dest[i] == NO_MOVE) {
             pb += sel_bytes(a, 0, false);
             continue;
@@ -246,6 +279,152 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, c
     if (a.prof && l == 0 && pb) atomicAdd(a.prof, pb);
 }
 
+// ---- degree classes for sub-warp groups ------------------------------------
+// The vertices of order1 bucket 0 (degree < 128) are split by degree into
+// class 0 (<= 8), 1 (<= 16), 2 (<= 32) and 3 (< 128) so that a warp can serve
+// 4, 2 or 1 low-degree vertices at once.  Order inside a class is irrelevant:
+// every consumer treats vertices independently.
+constexpr int NCLS = 4;
+__device__ __forceinline__ int deg_class(i64 d) { return d <= 8 ? 0 : (d <= 16 ? 1 : (d <= 32 ? 2 : 3)); }
+
+struct ClassLists {
+    i32* list = nullptr;          // [count] vertices grouped by class
+    i64* off = nullptr;           // [NCLS + 1] device class offsets
+    unsigned long long* cnt = nullptr;  // [2 * NCLS] device counters / cursors
+    i64 count = 0;                // host: number of listed vertices
+};
+
+__global__ void k_class_count(const i32* list, i64 count, const i64* rowptr, unsigned long long* cnt) {
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    const int l = lane_id();
+    for (i64 x0 = gw * 32; x0 < count; x0 += nw * 32) {
+        i64 x = x0 + l;
+        int k = -1;
+        if (x < count) {
+            i32 i = list[x];
+            k = deg_class(rowptr[i + 1] - rowptr[i]);
+        }
+        for (int c = 0; c < NCLS; c++) {
+            unsigned m = __ballot_sync(FULL, k == c);
+            if (l == 0 && m) atomicAdd(&cnt[c], (unsigned long long)__popc(m));
+        }
+    }
+}
+__global__ void k_class_offsets(unsigned long long* cnt, i64* off) {
+    i64 s = 0;
+    for (int c = 0; c < NCLS; c++) {
+        off[c] = s;
+        i64 v = (i64)cnt[c];
+        cnt[NCLS + c] = (unsigned long long)s;  // scatter cursor
+        s += v;
+    }
+    off[NCLS] = s;
+}
+__global__ void k_class_scatter(const i32* list, i64 count, const i64* rowptr, unsigned long long* cnt, i32* out) {
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    const int l = lane_id();
+    for (i64 x0 = gw * 32; x0 < count; x0 += nw * 32) {
+        i64 x = x0 + l;
+        int k = -1;
+        i32 i = -1;
+        if (x < count) {
+            i = list[x];
+            k = deg_class(rowptr[i + 1] - rowptr[i]);
+        }
+        for (int c = 0; c < NCLS; c++) {
+            unsigned m = __ballot_sync(FULL, k == c);
+            unsigned long long base = 0;
+            if (l == 0 && m) base = atomicAdd(&cnt[NCLS + c], (unsigned long long)__popc(m));
+            base = __shfl_sync(FULL, base, 0);
+            if (k == c) out[base + __popc(m & lanemask_lt())] = i;
+        }
+    }
+}
+
+// Builds the class lists of order1[0, off_large) into workspace slots.
+inline void build_class_lists(Context& ctx, const i64* rowptr, const Ordering& ord, int slot_list, int slot_off,
+                              int slot_cnt, ClassLists& cl) {
+    cl.count = ord.off_large;
+    cl.list = ctx.ws_get<i32>(slot_list, std::max<i64>(cl.count, 1));
+    cl.off = ctx.ws_get<i64>(slot_off, NCLS + 1);
+    cl.cnt = ctx.ws_get<unsigned long long>(slot_cnt, 2 * NCLS);
+    PGGC_CUDA(cudaMemsetAsync(cl.cnt, 0, sizeof(unsigned long long) * 2 * NCLS, ctx.stream));
+    int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(std::max<i64>(cl.count, 1), 256), (i64)ctx.num_sms * 8));
+    if (cl.count > 0) {
+        k_class_count<<<grid, 256, 0, ctx.stream>>>(ord.order1.p, cl.count, rowptr, cl.cnt);
+        PGGC_LAUNCH_CHECK();
+    }
+    k_class_offsets<<<1, 1, 0, ctx.stream>>>(cl.cnt, cl.off);
+    PGGC_LAUNCH_CHECK();
+    if (cl.count > 0) {
+        k_class_scatter<<<grid, 256, 0, ctx.stream>>>(ord.order1.p, cl.count, rowptr, cl.cnt, cl.list);
+        PGGC_LAUNCH_CHECK();
+    }
+}
+
+template <int G>
+__device__ __forceinline__ void group_best(Best& b) {
+#pragma unroll
+    for (int d = G / 2; d >= 1; d >>= 1) {
+        float oj = __shfl_xor_sync(FULL, b.jc, d);
+        i32 oc = __shfl_xor_sync(FULL, b.c, d);
+        if (better(oj, oc, b)) b = Best{oj, oc};
+    }
+}
+
+// G-lane groups, one vertex each, for vertices of degree <= G (single chunk):
+// class k of the class lists.
+template <class W, bool CON, int G>
+__global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls, const i64* off, int k) {
+    using V = typename Traits<W>::V;
+    constexpr int NG = 32 / G;
+    const int l = lane_id(), r = l & (G - 1), grp = l / G;
+    const i64 lo = off[k], hi = off[k + 1];
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    unsigned long long pb = 0;
+    for (i64 base = lo + gw * NG; base < hi; base += nw * NG) {
+        const i64 x = base + grp;
+        i32 i = -1;
+        bool act = false;
+        if (x < hi) {
+            i = cls[x];
+            act = a.dest[i] != NO_MOVE;
+        }
+        VCtx vc{};
+        i64 b = 0, e = 0;
+        if (act) {
+            vc = sel_prologue(a, i);
+            b = a.g.rowptr[i];
+            e = a.g.rowptr[i + 1];
+        }
+        if (r == 0 && x < hi) pb += sel_bytes(a, e - b, act);
+        Best best = none_best();
+        const i64 j = b + r;
+        const bool valid = act && j < e;
+        if (a.initial) {
+            if (valid) sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
+        } else {
+            i32 c = valid ? a.part[a.g.col[j]] : -1;
+            V wv = valid ? V(a.g.wgt(j)) : V(0);
+            bool keep = valid && c != vc.p;
+            u64 key = keep ? (((u64)grp << 32) | (u64)(u32)c) : (0xFFFFFFFF00000000ull | (u64)l);
+            unsigned peers = __match_any_sync(FULL, key);
+            bool leader = keep && ((peers & lanemask_lt()) == 0);
+            V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
+            if (leader) sel_eval<W, CON>(a, vc, c, s, best);
+        }
+        group_best<G>(best);
+        if (r == 0 && act) sel_finish(a, i, vc, best);
+    }
+    if (a.prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (l == 0 && pb) atomicAdd(a.prof, pb);
+    }
+}
+
 // ---- block per vertex (256 threads), shared or global table ----------------
 template <class W, bool CON, bool GLOBAL>
 __global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* list, i64 count, i32* gkeys,
@@ -254,7 +433,7 @@ __global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* l
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Best wb[8];
     V* svals = (V*)smem_raw;
-    i32* skeys = (i32*)(smem_raw + sizeof(V) * SEL_TS_MAX);
+    i32* skeys = (i32*)(smem_raw + sizeof(V) * (GLOBAL ? 0 : gcap));  // gcap = shared table slots
     const int l = lane_id(), w = threadIdx.x >> 5;
     i32* keys = GLOBAL ? gkeys + (i64)blockIdx.x * gcap : skeys;
     V* vals = GLOBAL ? gvals + (i64)blockIdx.x * gcap : svals;
@@ -335,38 +514,6 @@ __device__ __forceinline__ typename Traits<W>::V own_block1024(const DGraph<W>& 
     }
 }
 
-// mode 0: every vertex (natural order, skipping massive ones)
-// mode 1: only flagged vertices; also resets dest to NULL_PART and clears the flag
-template <class W>
-__global__ void __launch_bounds__(256) k_own_warp(DGraph<W> g, const i32* lab, typename Traits<W>::V* out, int mode,
-                                                  unsigned char* flags, i32* dest) {
-    const int l = lane_id();
-    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
-    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
-    for (i64 base = gw * 32; base < g.n; base += nw * 32) {
-        i64 v = base + l;
-        bool want = false;
-        if (v < g.n) {
-            bool small = (g.rowptr[v + 1] - g.rowptr[v]) < MASSIVE_CUTOFF;
-            want = small && (mode == 0 || flags[v]);
-        }
-        unsigned m = __ballot_sync(FULL, want);
-        while (m) {
-            int src = __ffs(m) - 1;
-            m &= m - 1;
-            i32 i = (i32)(base + src);
-            auto r = own_warp(g, lab, i);
-            if (l == 0) {
-                out[i] = r;
-                if (mode == 1) {
-                    dest[i] = NULL_PART;
-                    flags[i] = 0;
-                }
-            }
-        }
-    }
-}
-
 template <class W>
 __global__ void __launch_bounds__(1024) k_own_massive(DGraph<W> g, const i32* lab, typename Traits<W>::V* out,
                                                       const i32* list, i64 count, int mode, unsigned char* flags,
@@ -387,15 +534,84 @@ __global__ void __launch_bounds__(1024) k_own_massive(DGraph<W> g, const i32* la
     }
 }
 
+// G-lane groups over a vertex range; mode 0: every vertex, mode 1: flagged
+// vertices only (also resets their dest cache and clears the flag)
+template <class W, int G>
+__global__ void __launch_bounds__(256) k_own_grp(DGraph<W> g, const i32* lab, typename Traits<W>::V* out, Range rg,
+                                                 int mode, unsigned char* flags, i32* dest,
+                                                 unsigned long long* prof) {
+    using V = typename Traits<W>::V;
+    constexpr int NG = 32 / G;
+    const int l = lane_id(), r = l & (G - 1), grp = l / G;
+    const i64 lo = rg.begin(), hi = rg.end();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    unsigned long long pb = 0;
+    for (i64 base = lo + gw * NG; base < hi; base += nw * NG) {
+        const i64 x = base + grp;
+        i32 i = -1;
+        bool act = false;
+        if (x < hi) {
+            i = rg.list[x];
+            act = mode == 0 || flags[i];
+        }
+        i64 b = 0, e = 0;
+        i32 li = 0;
+        if (act) {
+            b = g.rowptr[i];
+            e = g.rowptr[i + 1];
+            li = lab[i];
+        }
+        V v = group_vsum<G, V>(b, e, r, [&](i64 j) -> V { return lab[g.col[j]] == li ? V(g.wgt(j)) : V(0); });
+        if (r == 0 && act) {
+            out[i] = v;
+            if (mode == 1) {
+                dest[i] = NULL_PART;
+                flags[i] = 0;
+            }
+            // list entry, offsets, own label, result; per edge column, weight, label
+            pb += 4 + 16 + 4 + sizeof(V) + (unsigned long long)(e - b) * (8 + (g.w ? sizeof(W) : 0));
+        }
+    }
+    if (prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (l == 0 && pb) atomicAdd(prof, pb);
+    }
+}
+
 template <class W>
 void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* lab,
-                      typename Traits<W>::V* out, int mode, unsigned char* flags, i32* dest) {
+                      typename Traits<W>::V* out, int mode, unsigned char* flags, i32* dest,
+                      const ClassLists* cls = nullptr) {
     auto gv = g.view();
     if (g.n == 0) return;
     ProfScope ps(ctx, "own_weights");
-    int grid = (int)std::min<i64>(ceil_div(ceil_div(g.n, 32), 8), (i64)ctx.num_sms * 16);
-    k_own_warp<W><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, mode, flags, dest);
-    PGGC_LAUNCH_CHECK();
+    unsigned long long* prof = ctx.prof_counter("own_weights");
+    ClassLists local;
+    if (!cls) {
+        build_class_lists(ctx, gv.rowptr, ord, WS_OWN_CLS, WS_OWN_OFF, WS_OWN_CNT, local);
+        cls = &local;
+    }
+    const i64 c01 = cls->count;  // host upper bound of every class range
+    if (c01 > 0) {
+        int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(c01, 32), (i64)ctx.num_sms * 16));
+        k_own_grp<W, 8><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 0, cls->off + 2),
+                                                       mode, flags, dest, prof);
+        PGGC_LAUNCH_CHECK();
+        k_own_grp<W, 16><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 2, cls->off + 3),
+                                                        mode, flags, dest, prof);
+        PGGC_LAUNCH_CHECK();
+        k_own_grp<W, 32><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 3, cls->off + 4),
+                                                        mode, flags, dest, prof);
+        PGGC_LAUNCH_CHECK();
+    }
+    if (ord.off_large2 > ord.off_large) {
+        int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(ord.off_large2 - ord.off_large, 8), (i64)ctx.num_sms * 16));
+        k_own_grp<W, 32><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
+                                                        host_range(ord.order1.p, ord.off_large, ord.off_large2), mode,
+                                                        flags, dest, prof);
+        PGGC_LAUNCH_CHECK();
+    }
     i64 nm = g.n - ord.off_large2;
     if (nm > 0) {
         int gb = (int)std::min<i64>(nm, (i64)ctx.num_sms * 2);
@@ -455,39 +671,62 @@ __device__ __forceinline__ double ab_term(const ABArgs<W>& a, i64 j, i32 p, i32 
     return 0.0;
 }
 
-template <class W>
-__global__ void __launch_bounds__(256) k_afterburner_warp(ABArgs<W> a) {
+// candidates (dest != NO_MOVE) of a vertex range, G-lane groups; keep is
+// indexed by vertex
+template <class W, int G>
+__global__ void __launch_bounds__(256) k_afterburner_grp(ABArgs<W> a, Range rg) {
+    constexpr int NG = 32 / G;
+    const int l = lane_id(), r = l & (G - 1), grp = l / G;
+    const i64 lo = rg.begin(), hi = rg.end();
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
-    const i64 hi_x = a.sc->split;
     unsigned long long pb = 0;
-    for (i64 x = gw; x < hi_x; x += nw) {
-        i32 i = a.cand[x];
-        i32 best = a.dest[i], p = a.part[i];
-        float multi = to_f(a.g.vtx_w[i]) * a.pm;
-        float igain = a.gain[i];
-        i32 hi = (i32)xorshift32((u32)i);
-        pb += ab_bytes(a, a.g.rowptr[i + 1] - a.g.rowptr[i]);
-        double ch = warp_canon_sum(a.g.rowptr[i], a.g.rowptr[i + 1],
-                                   [&](i64 j) { return ab_term(a, j, p, best, multi, igain, hi); });
-        if (lane_id() == 0) a.keep[x] = (igain + (float)ch) >= 0.0f ? 1 : 0;
+    for (i64 base = lo + gw * NG; base < hi; base += nw * NG) {
+        const i64 x = base + grp;
+        i32 i = -1;
+        bool act = false;
+        if (x < hi) {
+            i = rg.list[x];
+            act = a.dest[i] != NO_MOVE;
+        }
+        i32 best = 0, p = 0, hv = 0;
+        float multi = 0.f, igain = 0.f;
+        i64 b = 0, e = 0;
+        if (act) {
+            best = a.dest[i];
+            p = a.part[i];
+            multi = to_f(a.g.vtx_w[i]) * a.pm;
+            igain = a.gain[i];
+            hv = (i32)xorshift32((u32)i);
+            b = a.g.rowptr[i];
+            e = a.g.rowptr[i + 1];
+        }
+        double ch = group_vsum<G, double>(b, e, r, [&](i64 j) { return ab_term(a, j, p, best, multi, igain, hv); });
+        if (r == 0 && act) {
+            a.keep[i] = (igain + (float)ch) >= 0.0f ? 1 : 0;
+            pb += ab_bytes(a, e - b);
+        }
     }
-    if (a.prof && lane_id() == 0 && pb) atomicAdd(a.prof, pb);
+    if (a.prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (l == 0 && pb) atomicAdd(a.prof, pb);
+    }
 }
 
 template <class W>
-__global__ void __launch_bounds__(1024) k_afterburner_block(ABArgs<W> a) {
+__global__ void __launch_bounds__(1024) k_afterburner_block(ABArgs<W> a, Range rg) {
     __shared__ double red[32];
-    const i64 lo = a.sc->split, hi_x = a.sc->num_cand;
+    const i64 lo = rg.begin(), hi_x = rg.end();
     for (i64 x = lo + blockIdx.x; x < hi_x; x += gridDim.x) {
-        i32 i = a.cand[x];
+        i32 i = rg.list[x];
+        if (a.dest[i] == NO_MOVE) continue;
         i32 best = a.dest[i], p = a.part[i];
         float multi = to_f(a.g.vtx_w[i]) * a.pm;
         float igain = a.gain[i];
         i32 hi = (i32)xorshift32((u32)i);
         double ch = block1024_canon_sum(a.g.rowptr[i], a.g.rowptr[i + 1],
                                         [&](i64 j) { return ab_term(a, j, p, best, multi, igain, hi); }, red);
-        if (threadIdx.x == 0) a.keep[x] = (igain + (float)ch) >= 0.0f ? 1 : 0;
+        if (threadIdx.x == 0) a.keep[i] = (igain + (float)ch) >= 0.0f ? 1 : 0;
     }
 }
 
@@ -510,8 +749,9 @@ struct CandEpi {
     }
 };
 struct KeepFlag {
-    const unsigned char* keep;
-    __device__ i64 operator()(i64 x) const { return keep[x]; }
+    const i32* cand;
+    const unsigned char* keep;  // indexed by vertex
+    __device__ i64 operator()(i64 x) const { return keep[cand[x]]; }
 };
 // move-list compaction that also counts the NEW_PART moves
 struct MoveEpi {
@@ -599,9 +839,11 @@ __global__ void k_finish_new(LMScalars<V>* sc, i64 capacity) {
 // ---------------------------------------------------------------------------
 // perform_moves (src/local_mover.cpp:1241-1279)
 // ---------------------------------------------------------------------------
+// csize / moved_at (NULL unless the learned filter is on) track cluster sizes
+// and the sweep in which each vertex last moved
 template <class W>
 __global__ void k_apply_moves(DGraph<W> g, const i32* moves, i64 nm, const i32* dest, i32* part,
-                              typename Traits<W>::V* td, int* err) {
+                              typename Traits<W>::V* td, int* err, i32* csize, i32* moved_at, i32 stamp) {
     for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < nm; x += (i64)gridDim.x * blockDim.x) {
         i32 i = moves[x];
         i32 b = dest[i], p = part[i];
@@ -613,6 +855,11 @@ __global__ void k_apply_moves(DGraph<W> g, const i32* moves, i64 nm, const i32* 
         vatomic_add(&td[p], -w);
         vatomic_add(&td[b], w);
         part[i] = b;
+        if (csize) {
+            atomicSub(&csize[p], 1);
+            atomicAdd(&csize[b], 1);
+            moved_at[i] = stamp;
+        }
     }
 }
 
@@ -912,9 +1159,13 @@ struct Mover {
     View<V> gvals;
     i64 gcap = 0;
     bool cdata_init = false;
+    ClassLists cls;
+    // learned filter state (allocated only when the context's filter is on)
+    bool filt_on = false;
+    View<i32> moved_at, csize;
 
     enum Slot { S_PART, S_DEST, S_CAND, S_MOVES, S_NEWL, S_AVAIL, S_PRIO, S_GAIN, S_PV, S_PVC, S_TD, S_FLAGS, S_KEEP,
-                S_HAS, S_SC, S_GK, S_GV };
+                S_HAS, S_SC, S_GK, S_GV, S_CLS, S_CLS_OFF, S_CLS_CNT, S_MOVED_AT, S_CSIZE };
 
     Mover(Context& c, const Graph<W>& gr, const Ordering& o, i64 capacity)
         : ctx(c), g(gr), ord(o), n(gr.n), cap(capacity) {
@@ -934,12 +1185,76 @@ struct Mover {
         has.p = ctx.ws_get<unsigned char>(S_HAS, cc);
         sc.p = ctx.ws_get<LMScalars<V>>(S_SC, 1);
         PGGC_CUDA(cudaMemsetAsync(flags.p, 0, nn, ctx.stream));
+        build_class_lists(ctx, g.view().rowptr, ord, S_CLS, S_CLS_OFF, S_CLS_CNT, cls);
         if (ord.n_huge > 0) {
             gcap = next_pow2_u32((u32)std::min<i64>(2 * ord.max_deg, (i64)1 << 30));
             i64 nb = std::min<i64>(ord.n_huge, 32);
             gkeys.p = ctx.ws_get<i32>(S_GK, gcap * nb);
             gvals.p = ctx.ws_get<V>(S_GV, gcap * nb);
         }
+    }
+
+    // learned filter: per-call state once `part` holds the starting partition
+    void filter_init() {
+        filt_on = ctx.filt.mode != 0;
+        if (!filt_on) return;
+        i64 nn = std::max<i64>(n, 1), cc = std::max<i64>(cap, 1);
+        moved_at.p = ctx.ws_get<i32>(S_MOVED_AT, nn);
+        csize.p = ctx.ws_get<i32>(S_CSIZE, cc);
+        fill<i32>(ctx, moved_at.p, n, -1);
+        PGGC_CUDA(cudaMemsetAsync(csize.p, 0, sizeof(i32) * cc, ctx.stream));
+        PGGC_CUDA(cudaMemsetAsync(gain.p, 0, sizeof(float) * nn, ctx.stream));
+        k_cluster_sizes<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(part.p, n, csize.p);
+        PGGC_LAUNCH_CHECK();
+    }
+
+    // before a sweep's select: sample features (log mode) or drop the vertices
+    // the network rejects (filter mode)
+    void filter_pre(int sweep_idx, double vol_total) {
+        if (!filt_on) return;
+        auto& F = ctx.filt;
+        F.stamp++;
+        if (F.mode == 2 && F.suspended) return;
+        ProfScope ps(ctx, "filter");
+        FiltArgs<W> a;
+        a.g = g.view();
+        a.part = part.p;
+        a.pvals = pvals.p;
+        a.gain = gain.p;
+        a.moved_at = moved_at.p;
+        a.csize = csize.p;
+        a.td = td_curr.p;
+        a.dest = dest.p;
+        a.inv_vol = vol_total > 0 ? (float)(1.0 / vol_total) : 0.f;
+        a.inv_log_n = (float)(1.0 / std::log2(2.0 + (double)n));
+        a.level_f = (float)F.level / 16.f;
+        a.sweep_f = (float)sweep_idx / 8.f;
+        a.prev_stamp = F.stamp - 1;
+        a.mode = F.mode;
+        a.net = F.net;
+        a.threshold = F.threshold;
+        a.log_x = F.log_x;
+        a.log_v = F.log_v;
+        a.log_y = F.log_y;
+        a.log_cnt = F.log_cnt;
+        a.log_cap = F.log_cap;
+        a.rate = F.log_rate;
+        a.salt = (u32)(F.log_seed ^ ((u64)(u32)F.stamp * 0x9E3779B9ull));
+        a.stats = F.stats;
+        if (F.mode == 1)
+            PGGC_CUDA(cudaMemcpyAsync(F.log_cnt + 1, F.log_cnt, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                      ctx.stream));
+        int grid = grid_for(ctx, ceil_div(n, 32 * FW_WARPS), 1, 8);
+        k_filter_sweep<W><<<grid, FW_WARPS * 32, 0, ctx.stream>>>(a);
+        PGGC_LAUNCH_CHECK();
+    }
+
+    // after the afterburner: label this sweep's logged samples
+    void filter_post() {
+        if (!filt_on || ctx.filt.mode != 1) return;
+        auto& F = ctx.filt;
+        k_filter_label<<<ctx.num_sms, 256, 0, ctx.stream>>>(F.log_v, F.log_y, F.log_cnt, F.log_cap, dest.p, keep.p);
+        PGGC_LAUNCH_CHECK();
     }
 
     SelArgs<W> sel_args(float fr, bool initial, const i32* constraint, const V* td, const i32* partp,
@@ -962,24 +1277,41 @@ struct Mover {
         return a;
     }
 
+    i64 label_bound_host = 0;  // host upper bound of the label count (table sizing)
+
     template <bool CON>
     void launch_select_t(SelArgs<W> a) {
         if (ord.off_large > 0) {
             ProfScope ps(ctx, "select_warp");
             a.prof = ctx.prof_counter("select_warp");
+            int grid_g = grid_for(ctx, ceil_div(cls.count, 32), 1, 16);
+            k_select_grp<W, CON, 8><<<grid_g, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 0);
+            PGGC_LAUNCH_CHECK();
+            k_select_grp<W, CON, 16><<<grid_g, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 1);
+            PGGC_LAUNCH_CHECK();
+            k_select_grp<W, CON, 32><<<grid_g, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 2);
+            PGGC_LAUNCH_CHECK();
             int grid = grid_for(ctx, ceil_div(ord.off_large, SELW_WARPS), 1, 16);
-            k_select_warp<W, CON><<<grid, SELW_WARPS * 32, 0, ctx.stream>>>(a, ord.order1.p, ord.off_large);
+            k_select_warp<W, CON><<<grid, SELW_WARPS * 32, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 3,
+                                                                                          cls.off + 4));
             PGGC_LAUNCH_CHECK();
         }
         i64 nb = n - ord.off_large;
         if (nb > 0) {
             ProfScope ps(ctx, "select_block");
             a.prof = ctx.prof_counter("select_block");
-            size_t sm = (sizeof(V) + sizeof(i32)) * SEL_TS_MAX;
-            set_dynamic_smem_once(k_select_block<W, CON, false>, (int)sm, ctx.device);
-            int grid = (int)std::min<i64>(nb, (i64)ctx.num_sms * 2);
+            // shared table sized to the largest table a vertex of this bucket can need
+            i64 umax = std::max<i64>(1, std::min<i64>(std::min<i64>(ord.max_deg, HUGE_DEG),
+                                                      label_bound_host > 0 ? label_bound_host : HUGE_DEG));
+            i64 tmax = next_pow2_u32((u32)(2 * umax));
+            size_t sm = (sizeof(V) + sizeof(i32)) * (size_t)tmax;
+            set_dynamic_smem_once(k_select_block<W, CON, false>, (int)((sizeof(V) + sizeof(i32)) * SEL_TS_MAX),
+                                  ctx.device);
+            int per_sm = 0;
+            PGGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_block<W, CON, false>, 256, sm));
+            int grid = (int)std::min<i64>(nb, (i64)ctx.num_sms * std::max(per_sm, 1));
             k_select_block<W, CON, false><<<grid, 256, sm, ctx.stream>>>(a, ord.order1.p + ord.off_large, nb, nullptr,
-                                                                         nullptr, 0);
+                                                                         nullptr, tmax);
             PGGC_LAUNCH_CHECK();
         }
         if (ord.n_huge > 0) {
@@ -1018,22 +1350,35 @@ struct Mover {
         a.keep = keep.p;
         a.sc = sc.p;
         a.prof = ctx.prof_counter("afterburner_warp");
-        int grid = grid_for(ctx, ceil_div(n, 8), 1, 16);
         {
             ProfScope ps(ctx, "afterburner_warp");
-            k_afterburner_warp<W><<<grid, 256, 0, ctx.stream>>>(a);
-            PGGC_LAUNCH_CHECK();
+            if (cls.count > 0) {
+                int grid = grid_for(ctx, ceil_div(cls.count, 32), 1, 16);
+                k_afterburner_grp<W, 8><<<grid, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 0, cls.off + 2));
+                PGGC_LAUNCH_CHECK();
+                k_afterburner_grp<W, 16><<<grid, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 2, cls.off + 3));
+                PGGC_LAUNCH_CHECK();
+                k_afterburner_grp<W, 32><<<grid, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 3, cls.off + 4));
+                PGGC_LAUNCH_CHECK();
+            }
+            if (ord.off_large2 > ord.off_large) {
+                int grid = grid_for(ctx, ceil_div(ord.off_large2 - ord.off_large, 8), 1, 16);
+                k_afterburner_grp<W, 32><<<grid, 256, 0, ctx.stream>>>(
+                    a, host_range(ord.order1.p, ord.off_large, ord.off_large2));
+                PGGC_LAUNCH_CHECK();
+            }
         }
         i64 nm = n - ord.off_large2;
         if (nm > 0) {
             ProfScope ps(ctx, "afterburner_block");
             a.prof = nullptr;
-            k_afterburner_block<W><<<(int)std::min<i64>(nm, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(a);
+            k_afterburner_block<W><<<(int)std::min<i64>(nm, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(
+                a, host_range(ord.order1.p, ord.off_large2, n));
             PGGC_LAUNCH_CHECK();
         }
         PGGC_CUDA(cudaMemsetAsync(&sc.p->new_hint, 0, sizeof(unsigned long long), ctx.stream));
-        scan_apply(ctx, KeepFlag{keep.p}, MoveEpi{cand.p, dest.p, moves.p, &sc.p->new_hint}, n, &sc.p->num_cand,
-                   &sc.p->num_moves);
+        scan_apply(ctx, KeepFlag{cand.p, keep.p}, MoveEpi{cand.p, dest.p, moves.p, &sc.p->new_hint}, n,
+                   &sc.p->num_cand, &sc.p->num_moves);
     }
 
     void set_new_cluster_ids(i64 nmoves_host, i32* constraint) {
@@ -1055,17 +1400,18 @@ struct Mover {
 
     void perform_moves(i64 nm, double lambda, i64 label_bound) {
         auto gv = g.view();
-        k_apply_moves<W><<<grid_for(ctx, nm, 256), 256, 0, ctx.stream>>>(gv, moves.p, nm, dest.p, part.p, td_curr.p,
-                                                                        ctx.d_err);
+        k_apply_moves<W><<<grid_for(ctx, nm, 256), 256, 0, ctx.stream>>>(
+            gv, moves.p, nm, dest.p, part.p, td_curr.p, ctx.d_err, filt_on ? csize.p : nullptr,
+            filt_on ? moved_at.p : nullptr, ctx.filt.stamp);
         PGGC_LAUNCH_CHECK();
         if (!cdata_init) {
             cdata_init = true;
-            own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 0, nullptr, nullptr);
+            own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 0, nullptr, nullptr, &cls);
             fill<i32>(ctx, dest.p, n, NULL_PART);
         } else {
             k_mark_affected<W><<<grid_for(ctx, ceil_div(nm, 8), 1, 16), 256, 0, ctx.stream>>>(gv, moves.p, nm, flags.p);
             PGGC_LAUNCH_CHECK();
-            own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 1, flags.p, dest.p);
+            own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 1, flags.p, dest.p, &cls);
         }
         update_objective_dev(lambda, label_bound);
     }
@@ -1182,9 +1528,10 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
     copy_d2d(ctx, m.part.p, best_part, n);
     copy_d2d(ctx, m.td_curr.p, best.total_deg.p, best.label_count);
     fill<i32>(ctx, m.dest.p, n, NULL_PART);
+    if (!strict) m.filter_init();
     if (!is_initial) {
         m.cdata_init = true;
-        own_weights_impl<W>(ctx, g, ord, m.part.p, m.pvals.p, 0, nullptr, nullptr);
+        own_weights_impl<W>(ctx, g, ord, m.part.p, m.pvals.p, 0, nullptr, nullptr, &m.cls);
     } else {
         m.cdata_init = false;
         PGGC_CUDA(cudaMemsetAsync(m.pvals.p, 0, sizeof(V) * n, ctx.stream));
@@ -1212,11 +1559,14 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
                 if (!budget()) break;
                 sweeps++;
                 iter_count++;
+                m.filter_pre(iter_count - 1, best.vol_total);
                 auto a = m.sel_args(fr, !m.cdata_init, constraint, m.td_curr.p, m.part.p, m.pvals.p, m.dest.p,
                                     m.gain.p, &m.sc.p->label_count, pm);
+                m.label_bound_host = label_bound;
                 m.launch_select(a, constrained);
                 m.compact_candidates();
                 m.afterburner(pm);
+                m.filter_post();
                 const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
                 i64 ncand = hs->num_cand, nm = hs->num_moves;
                 const bool any_new = hs->new_hint != 0;
@@ -1236,6 +1586,7 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
             sweeps++;
             auto a = m.sel_args(0.0f, !m.cdata_init, constraint, m.td_curr.p, m.part.p, m.pvals.p, m.dest.p, m.gain.p,
                                 &m.sc.p->label_count, pm);
+            m.label_bound_host = label_bound;
             m.launch_select(a, constrained);
             m.compact_candidates();
             const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
@@ -1278,6 +1629,7 @@ i64 select_pass(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32*
     PGGC_CUDA(cudaMemcpyAsync(m.sc.p, &h, sizeof(h), cudaMemcpyHostToDevice, ctx.stream));
     auto a = m.sel_args(filter_ratio, initial, constraint, cs.total_deg.p, part, pvals, dest, gain,
                         &m.sc.p->label_count, (float)cs.lambda);
+    m.label_bound_host = cs.label_count;
     m.launch_select(a, constrained);
     scan_apply(ctx, CandFlag{ord.order1.p, dest}, CandEpi{ord.order1.p, m.cand.p, -1, nullptr}, g.n, nullptr,
                &m.sc.p->num_cand);
