@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--cpu-sample-n", type=int, default=262144)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--batched-learned", type=int, default=0, metavar="K",
+                    help="also time a population of K seeds run concurrently (pggc_batch_run) with the learned "
+                         "move filter, trained first on logs of plain runs of smaller graphs")
     ap.add_argument("--ex-iters", type=int, default=-1,
                     help="pLeiden+ passes after the first (-1: until the objective stops rising)")
     return ap.parse_args()
@@ -293,6 +296,9 @@ def ours(args):
             import torch.distributed as dist
             dist.destroy_process_group()
         return
+    bl = None
+    if args.batched_learned > 0:
+        bl = batched_learned(args, pg, mem, wg, m, q)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -315,10 +321,57 @@ def ours(args):
         "clocks": clk,
         "gpu_launches": int(launches),
     }
+    if bl is not None:
+        line["batched_learned"] = bl
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def batched_learned(args, pg, mem, wg, m, q_plain):
+    """Population of K seeds on the workload graph, concurrently on K streams,
+    with the learned move filter trained on logs of plain runs of 262,144-vertex
+    DC-SBMs (seeds 101-104, one pass each)."""
+    from pennsylvaniagpugraphclustering_b200 import graphgen as gg, move_filter as MF
+    t0 = time.perf_counter()
+    xs, ys = [], []
+    for s in (1, 2, 3, 4):
+        h = gg.dcsbm(262144, 100 + s)
+        g2 = pg.weighted_graph(mem, h.rowptr, h.col, h.w, objective=pg.OBJ_WMOD)
+        MF.log_start(mem, capacity=2_000_000, sample_rate=0.25, seed=s)
+        cd = pg.get_objective(mem, g2, pg.OBJ_WMOD, 1.0)
+        pg.run_clustering(mem, g2, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=s)
+        x, y, _ = MF.log_stop(mem, 2_000_000)
+        xs.append(x)
+        ys.append(y)
+        cd.close()
+        g2.close()
+    x = np.concatenate(xs)
+    y = np.concatenate(ys)
+    pos_w = float(min(20.0, (len(y) - y.sum()) / max(y.sum(), 1.0)))
+    params, losses = MF.train(mem, MF.init_params(1), x, y, epochs=6, batch=4096, lr=3e-3, pos_weight=pos_w)
+    thr = MF.threshold_for_recall(mem, params, x, y, recall=0.98)
+    train_s = time.perf_counter() - t0
+    K = args.batched_learned
+    jobs = [dict(graph=wg, objective=pg.OBJ_WMOD, method=pg.METHOD_LEIDEN_PLUS, ex_iters=args.ex_iters,
+                 seed=args.seed + k) for k in range(K)]
+    MF.enable(mem, params, thr)
+    try:
+        pg.batch_run(mem, jobs, streams=K)  # warm-up (worker streams, scratch)
+        MF.stats(mem, reset=True)
+        t1 = time.perf_counter()
+        res = pg.batch_run(mem, jobs, streams=K)
+        dt = time.perf_counter() - t1
+        ev, sk = MF.stats(mem)
+    finally:
+        MF.disable(mem)
+    qs = [st["objective"] for _, st in res]
+    return {"value": K * m / dt, "unit": UNIT, "population": K, "streams": K, "seconds": dt,
+            "modularity_mean": statistics.mean(qs), "modularity_min": min(qs), "plain_modularity": q_plain,
+            "filter_skipped_frac": sk / max(ev + sk, 1), "train_rows": int(len(y)), "train_seconds": train_s,
+            "final_train_loss": float(losses[-1]), "threshold_logit": thr,
+            "timing": "host wall clock around pggc_batch_run (all streams joined)"}
 
 
 def main():

@@ -180,6 +180,31 @@ pggc_status pggc_louvain_part(pggc_context* ctx, const pggc_graph* g, pggc_clust
 pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_cluster_data* cd, int method,
                                 int ex_iters, uint64_t seed, int32_t* labels_out, int mem_kind, pggc_stats* stats);
 
+/* ---- batched clustering (no counterpart in the reference) ------------------
+ * `count` independent run_clustering jobs -- a population of seeds on one graph
+ * (the memetic driver's population, app/memetic_clustering.cpp:118-219) or a
+ * set of uneven-size graphs -- run concurrently on `streams` CUDA streams of
+ * the context's device, one host thread per stream pulling jobs in order.
+ * Graphs must belong to `ctx`; each job builds its own cluster_data
+ * (objective, lambda_mult) and writes labels_out (n int32, host or device per
+ * mem_kind), stats and status.  A learned filter enabled on `ctx` applies to
+ * every job.  Returns the first failing job's status (its message in
+ * pggc_last_error) or PGGC_OK.  Results equal those of sequential
+ * pggc_run_clustering calls with the same arguments. */
+typedef struct pggc_batch_job {
+    const pggc_graph* graph;
+    int objective;
+    double lambda_mult;
+    int method;
+    int ex_iters;
+    uint64_t seed;
+    int32_t* labels_out;
+    int mem_kind;
+    pggc_stats stats; /* out */
+    int status;       /* out: pggc_status */
+} pggc_batch_job;
+pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, int streams);
+
 /* verify_objective<uniform> (app/verify_objective.cpp:64-89) in int64 / FP64 */
 pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, int objective,
                                   double lambda_mult, int mem_kind, double* objective_out, double* raw_obj_out);

@@ -5,7 +5,8 @@ contraction, Leiden refinement and the multilevel V-cycles that drive them --
 is hand-written CUDA in ``csrc/`` behind the C ABI of ``include/pggc.h``.
 :mod:`.api` mirrors the reference's host interface on top of that ABI.
 """
-from .api import (NEW_PART, NO_MOVE, NULL_PART, OBJECTIVES, build_coarse_graph, cluster_data, clustering_methods,
+from .api import (NEW_PART, NO_MOVE, NULL_PART, OBJECTIVES, batch_run, build_coarse_graph, cluster_data,
+                  clustering_methods,
                   coarsen_leidenR, constant_potts, generate_orderings, get_objective, local_move, local_move_strict,
                   memory_store, modularity, normalized_lcc, run_clustering, select_pass, verify_objective,
                   weighted_graph)

@@ -42,6 +42,13 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchJob(ctypes.Structure):
+    _fields_ = [("graph", ctypes.c_void_p), ("objective", ctypes.c_int), ("lambda_mult", ctypes.c_double),
+                ("method", ctypes.c_int), ("ex_iters", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("labels_out", ctypes.c_void_p), ("mem_kind", ctypes.c_int), ("stats", Stats),
+                ("status", ctypes.c_int)]
+
+
 # name -> (restype, argtypes)
 _vp, _i64, _ci, _dbl, _u32, _u64, _flt = (ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float)
@@ -77,6 +84,7 @@ _SIGS = {
     "pggc_filter_log_stop": (_ci, [_vp, _vp, _vp, _i64, _ci, ctypes.POINTER(_i64)]),
     "pggc_filter_enable": (_ci, [_vp, _vp, _flt]),
     "pggc_filter_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _ci]),
+    "pggc_batch_run": (_ci, [_vp, _vp, _i64, _ci]),
     "pggc_local_move": (_ci, [_vp, _vp, _vp, _vp, _ci, _ci, _vp, _i64, _ci, _ci, _ci, _ci, ctypes.POINTER(Stats)]),
     "pggc_select_pass": (_ci, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _flt, _ci, _ci, _vp, _ci, ctypes.POINTER(_i64)]),
     "pggc_build_coarse_graph": (_ci, [_vp, _vp, _vp, _i64, _ci, _PP]),

@@ -116,6 +116,7 @@ class weighted_graph:
     def __init__(self, mem: memory_store, rowptr, col, weights=None, objective: int = OBJ_MOD, vtx_w=None,
                  edge_uniform: Optional[bool] = None, _handle=None):
         self.mem = mem
+        self.objective = objective
         if _handle is not None:
             self._h = _handle
         else:
@@ -394,3 +395,29 @@ def run_clustering(mem, g, rfd, method=METHOD_LEIDEN_PLUS, ex_iters=0, seed=1, o
     check(L.lib().pggc_run_clustering(mem.handle, g.handle, rfd.handle, method, ex_iters, seed, lp, mk,
                                       ctypes.byref(st)))
     return labels, _stats_dict(st)
+
+
+def batch_run(mem: memory_store, jobs, streams: int = 8):
+    """Run independent clustering jobs concurrently (``pggc_batch_run``).
+
+    ``jobs`` is a list of dicts with keys ``graph`` (a :class:`weighted_graph`
+    of ``mem``), and optionally ``objective`` (default: the graph's),
+    ``lambda_mult`` (1.0), ``method`` (pLeiden+), ``ex_iters`` (0) and
+    ``seed`` (1).  Returns a list of (labels, stats dict) in job order.
+    """
+    arr = (L.BatchJob * max(len(jobs), 1))()
+    outs = []
+    for k, j in enumerate(jobs):
+        g = j["graph"]
+        lab = np.empty(max(g.n, 1), np.int32)
+        outs.append(lab)
+        arr[k].graph = g.handle
+        arr[k].objective = int(j.get("objective", g.objective))
+        arr[k].lambda_mult = float(j.get("lambda_mult", 1.0))
+        arr[k].method = int(j.get("method", METHOD_LEIDEN_PLUS))
+        arr[k].ex_iters = int(j.get("ex_iters", 0))
+        arr[k].seed = int(j.get("seed", 1))
+        arr[k].labels_out = lab.ctypes.data
+        arr[k].mem_kind = MEM_HOST
+    check(L.lib().pggc_batch_run(mem.handle, ctypes.cast(arr, ctypes.c_void_p), len(jobs), int(streams)))
+    return [(outs[k][:jobs[k]["graph"].n], _stats_dict(arr[k].stats)) for k in range(len(jobs))]

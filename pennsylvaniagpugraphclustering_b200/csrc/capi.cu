@@ -1,6 +1,7 @@
 // capi.cu -- the extern "C" boundary declared in include/pggc.h.
 #include <cstring>
 #include <string>
+#include <thread>
 #include "kernels.cuh"
 #include "mlp_train.cuh"
 #include "pggc.h"
@@ -17,6 +18,9 @@ std::atomic<unsigned long long> g_kernel_launches{0};
 struct pggc_context {
     std::unique_ptr<Context> ctx;
     std::atomic<int> refs{1};
+    // extra streams for pggc_batch_run, created on first use and kept
+    std::mutex workers_mu;
+    std::vector<std::unique_ptr<Context>> workers;
 };
 
 static void ctx_retain(pggc_context* c) { c->refs.fetch_add(1); }
@@ -680,47 +684,96 @@ pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_clu
         Context& c = *ctx->ctx;
         dispatch(g, [&](auto& gr, auto* vtag) {
             using V = std::remove_pointer_t<decltype(vtag)>;
+            using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
             auto& cs = cstate<V>(cd);
-            const i64 n = gr.n;
-            Out<i32> lab(c, labels_out, n, mem_kind, false);
-            DBuf<i32> part(c, std::max<i64>(n, 1)), con(c, std::max<i64>(n, 1));
+            Out<i32> lab(c, labels_out, gr.n, mem_kind, false);
             RunStats rs;
-            u64 pass = 0;
-            auto one = [&](bool improve) {
-                RunStats r1;
-                if (method == PGGC_METHOD_LOUVAIN) {
-                    louvain_part(c, gr, cs, improve, con.p, part.p, &r1);
-                } else {
-                    u64 s = seed + 0x9E3779B97F4A7C15ull * pass;
-                    pass++;
-                    leiden_part(c, gr, cs, method == PGGC_METHOD_LEIDEN_PLUS, improve, con.p, s, part.p, &r1);
-                }
-                rs.levels = r1.levels;
-                rs.total_nnz = r1.total_nnz;
-                rs.sweeps += r1.sweeps;
-                rs.moves += r1.moves;
-                rs.passes++;
-            };
-            one(false);
-            double last = -std::numeric_limits<double>::infinity();
-            int counter = 0;
-            while (true) {
-                bool terminate = true;
-                if (ex_iters < 0) {
-                    if (cs.get_objective() > last) terminate = false;
-                    last = cs.get_objective();
-                } else {
-                    if (counter++ < ex_iters) terminate = false;
-                }
-                if (terminate) break;
-                copy_d2d(c, con.p, part.p, n);
-                one(true);
-            }
-            copy_d2d(c, lab.p, part.p, n);
+            run_clustering<W>(c, gr, cs, method, ex_iters, seed, lab.p, &rs);
             lab.finish();
             c.sync();
             fill_stats(stats, rs, cs.get_objective(), cs.obj, cs.label_count);
         });
+    });
+}
+
+pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, int streams) {
+    return guarded([&] {
+        need(ctx && (count == 0 || jobs), "NULL argument");
+        need(count >= 0 && streams >= 1 && streams <= 64, "count must be >= 0 and streams in [1, 64]");
+        Context& c = *ctx->ctx;
+        for (i64 k = 0; k < count; k++) {
+            const auto& J = jobs[k];
+            need(J.graph && J.labels_out, "a job has a NULL graph or labels_out");
+            need(J.graph->owner == ctx, "a job's graph belongs to another context");
+            need(J.method >= PGGC_METHOD_LOUVAIN && J.method <= PGGC_METHOD_LEIDEN_PLUS, "unknown method");
+            need(J.objective >= PGGC_OBJ_MOD && J.objective <= PGGC_OBJ_LCC, "unknown objective");
+            check_mem_kind(J.mem_kind);
+        }
+        need(c.filt.mode != 1, "sample logging is not supported in batched runs");
+        if (count == 0) return;
+        c.sync();
+        const int nw = (int)std::min<i64>(streams, count);
+        {
+            std::lock_guard<std::mutex> lk(ctx->workers_mu);
+            while ((int)ctx->workers.size() < nw) ctx->workers.push_back(std::make_unique<Context>(c.device));
+        }
+        std::atomic<i64> next{0};
+        std::vector<std::string> msgs((size_t)count);
+        auto work = [&](int wi) {
+            Context& wc = *ctx->workers[wi];
+            cudaSetDevice(wc.device);
+            // the main context's learned filter (network, threshold, counters) is shared read-only
+            wc.filt.mode = c.filt.mode;
+            wc.filt.net = c.filt.net;
+            wc.filt.threshold = c.filt.threshold;
+            wc.filt.stats = c.filt.stats;
+            for (;;) {
+                const i64 k = next.fetch_add(1);
+                if (k >= count) break;
+                pggc_batch_job& J = jobs[k];
+                J.status = PGGC_ERR_INTERNAL;
+                try {
+                    dispatch(J.graph, [&](auto& gr, auto* vtag) {
+                        using V = std::remove_pointer_t<decltype(vtag)>;
+                        using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
+                        ClusterState<V> cs;
+                        make_cluster_state<W>(wc, gr, J.objective, J.lambda_mult, cs);
+                        Out<i32> lab(wc, J.labels_out, gr.n, J.mem_kind, false);
+                        RunStats rs;
+                        run_clustering<W>(wc, gr, cs, J.method, J.ex_iters, J.seed, lab.p, &rs);
+                        lab.finish();
+                        wc.sync();
+                        fill_stats(&J.stats, rs, cs.get_objective(), cs.obj, cs.label_count);
+                    });
+                    J.status = PGGC_OK;
+                } catch (const InvalidArg& e) {
+                    J.status = PGGC_ERR_INVALID;
+                    msgs[k] = e.what();
+                } catch (const DeviceFault& e) {
+                    J.status = PGGC_ERR_DEVICE;
+                    msgs[k] = e.what();
+                } catch (const CudaError& e) {
+                    J.status = PGGC_ERR_CUDA;
+                    msgs[k] = e.what();
+                } catch (const std::exception& e) {
+                    msgs[k] = e.what();
+                }
+            }
+            wc.filt.mode = 0;
+            wc.filt.net = nullptr;
+            wc.filt.stats = nullptr;
+        };
+        std::vector<std::thread> th;
+        for (int wi = 0; wi < nw; wi++) th.emplace_back(work, wi);
+        for (auto& t : th) t.join();
+        for (i64 k = 0; k < count; k++) {
+            if (jobs[k].status == PGGC_OK) continue;
+            std::string m = "batch job " + std::to_string(k) + ": " + msgs[k];
+            if (jobs[k].status == PGGC_ERR_INVALID) throw InvalidArg(m);
+            if (jobs[k].status == PGGC_ERR_DEVICE) throw DeviceFault(m);
+            if (jobs[k].status == PGGC_ERR_CUDA) throw CudaError(cudaErrorUnknown, m);
+            throw std::runtime_error(m);
+        }
     });
 }
 

@@ -5,15 +5,19 @@
 //     (sum of member degrees) of every coarse vertex;
 //  2. scans give member offsets and per-coarse-vertex scratch offsets; members
 //     are scattered (counting sort by coarse id) and their degrees prefix-summed
-//     so each coarse vertex owns one flat virtual edge list;
-//  3. hashed merge of the (c_u, c_v) keys: a warp per coarse vertex with bound
-//     <= 128 (per-warp shared-memory table, __match_any_sync chunk
-//     pre-aggregation), a 256-thread block for bound <= 4096 (shared-memory
-//     table), a block with a global-memory table above that; self-loops are
-//     dropped (src/contract.cpp:191,209) and weights summed exactly (int64 /
-//     FP64);
-//  4. a prefix sum of the unique counts gives the coarse row offsets;
-//  5. each row is sorted by column (warp rank sort, block bitonic sort in shared
+//     so each coarse vertex owns one flat member-edge list;
+//  3. flattening: one coalesced pass over the CSR writes every edge's coarse
+//     key (or -1 inside the coarse vertex: dropped self-loops,
+//     src/contract.cpp:191,209) and weight at its flat position;
+//  4. one pass sorts the rows into buckets; hashed merge of the keys reads each
+//     row as a contiguous stream: a warp per row with bound <= 256 (per-warp
+//     shared table, __match_any_sync chunk pre-aggregation), a block with a
+//     2048- or 8192-slot shared table up to 4096 distinct candidates, a
+//     1024-thread block with a 16384-slot shared table above that, and a block
+//     with a global table for the rows that overflow it; weights are summed
+//     exactly (int64 / FP64);
+//  5. a prefix sum of the unique counts gives the coarse row offsets;
+//  6. each row is sorted by column (warp rank sort, block bitonic sort in shared
 //     memory, LSD radix sort for rows above 4096 entries) and written out.
 // The output is the canonical (row, col)-sorted coarse CSR.
 #include "kernels.cuh"
@@ -32,11 +36,72 @@ __global__ void k_contract_count(DGraph<W> g, const i32* vcmap, i64* cnt, i64* b
     }
 }
 
-__global__ void k_scatter_members(const i32* vcmap, i64 n, i64* cursor, i32* members) {
+__global__ void k_scatter_members(const i32* vcmap, i64 n, i64* cursor, i32* members, i64* memberpos) {
     for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
         i32 c = vcmap[i];
         i64 pos = (i64)::atomicAdd((unsigned long long*)&cursor[c], 1ull);
         members[pos] = (i32)i;
+        memberpos[i] = pos;
+    }
+}
+
+// Flattening: every fine edge (u, v) is written once, at its position in its
+// coarse row's flat member-edge list (P[memberpos[u]] + rank within u's row),
+// as the coarse key vcmap[v] (-1 for an edge inside the coarse vertex, a
+// self-loop of the coarse graph) and its weight.  A warp streams the edge range
+// of 32 consecutive vertices with coalesced loads; each lane finds its edge's
+// source among the 32 by a 5-step shuffle search of the row offsets.  After
+// this pass the hashing kernels read their rows as contiguous streams.
+template <class W>
+__global__ void __launch_bounds__(256) k_flatten(DGraph<W> g, const i32* vcmap, const i64* P, const i64* memberpos,
+                                                 i32* fkey, W* fw) {
+    const int l = lane_id();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 u0 = gw * 32; u0 < g.n; u0 += nw * 32) {
+        const i64 uu = u0 + l;
+        const bool has = uu < g.n;
+        const i64 R = has ? g.rowptr[uu] : (i64)1 << 62;  // row start of the lane's vertex
+        const i64 B = has ? P[memberpos[uu]] : 0;          // its flat base
+        const i32 C = has ? vcmap[uu] : -1;                // its coarse id
+        const i64 e0 = g.rowptr[u0];
+        const i64 e1 = g.rowptr[min(u0 + 32, g.n)];
+        // FL_UNROLL chunks of 32 edges per iteration: their loads are issued
+        // together so that several gathers are in flight per warp
+        constexpr int FL_UNROLL = 4;
+        for (i64 j0 = e0; j0 < e1; j0 += 32 * FL_UNROLL) {
+            i32 col[FL_UNROLL];
+            W wv[FL_UNROLL];
+#pragma unroll
+            for (int k = 0; k < FL_UNROLL; k++) {
+                const i64 j = j0 + 32 * k + l;
+                col[k] = j < e1 ? g.col[j] : 0;
+                wv[k] = (g.w && j < e1) ? g.w[j] : W(0);
+            }
+            i32 cv[FL_UNROLL];
+#pragma unroll
+            for (int k = 0; k < FL_UNROLL; k++) cv[k] = j0 + 32 * k + l < e1 ? vcmap[col[k]] : 0;
+#pragma unroll
+            for (int k = 0; k < FL_UNROLL; k++) {
+                const i64 j = j0 + 32 * k + l;
+                // largest L with R_L <= j (vertices with no edges share R with the next)
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int cand = lo + step;
+                    const i64 rc = __shfl_sync(FULL, R, cand & 31);
+                    if (cand < 32 && rc <= j) lo = cand;
+                }
+                const i64 rs = __shfl_sync(FULL, R, lo);
+                const i64 bs = __shfl_sync(FULL, B, lo);
+                const i32 cs = __shfl_sync(FULL, C, lo);
+                if (j < e1) {
+                    const i64 q = bs + (j - rs);
+                    fkey[q] = cv[k] == cs ? -1 : cv[k];
+                    if (g.w) fw[q] = wv[k];
+                }
+            }
+        }
     }
 }
 
@@ -59,24 +124,14 @@ struct CArgs {
     const i64* cstart;   // member offsets [nc+1]
     const i32* members;
     const i64* P;        // exclusive prefix of member degrees in member order [n+1]
+    const i32* fkey;     // flattened coarse keys (-1: inside the coarse vertex) [nnz]
+    const W* fw;         // flattened weights [nnz] (unused for unit weights)
     i32* out_key;        // scratch, indexed by P[cstart[c]] + k
     V* out_val;
     i64* ucount;         // unique neighbours per coarse vertex
     int* err;
     u32 probe_cap;       // fault-injection cap on hash probes (0: none)
 };
-
-// Edge position j of virtual edge q (global flat index) of coarse vertex c.
-__device__ __forceinline__ i64 flat_edge(const i64* P, const i32* members, const i64* rowptr, i64 m0, i64 m1, i64 q) {
-    // largest m in [m0, m1) with P[m] <= q
-    i64 lo = m0, hi = m1 - 1;
-    while (lo < hi) {
-        i64 mid = (lo + hi + 1) >> 1;
-        if (P[mid] <= q) lo = mid;
-        else hi = mid - 1;
-    }
-    return rowptr[members[lo]] + (q - P[lo]);
-}
 
 template <class V>
 __device__ __forceinline__ void ctable_add(i32* keys, V* vals, u32 mask, i32 c, V x, int* err, u32 cap) {
@@ -101,6 +156,32 @@ __device__ __forceinline__ void ctable_add(i32* keys, V* vals, u32 mask, i32 c, 
     atomicExch(err, (int)DEV_ERR_PROBE);
 }
 
+// insert that gives up after CT_TRY_PROBES probes instead of latching an error
+// (the caller falls back to a larger table); a run that long means the table
+// is close to full, where further probing would cost O(table) per insert
+constexpr u32 CT_TRY_PROBES = 64;
+template <class V>
+__device__ __forceinline__ bool ctable_try_add(i32* keys, V* vals, u32 mask, i32 c, V x) {
+    u32 s = xorshift32((u32)c) & mask;
+    volatile i32* vk = keys;
+    for (u32 probe = 0; probe < CT_TRY_PROBES && probe <= mask; probe++) {
+        i32 k = vk[s];
+        if (k == c) {
+            cvatomic_add(&vals[s], x);
+            return true;
+        }
+        if (k == -1) {
+            i32 old = atomicCAS(&keys[s], -1, c);
+            if (old == -1 || old == c) {
+                cvatomic_add(&vals[s], x);
+                return true;
+            }
+        }
+        s = (s + 1) & mask;
+    }
+    return false;
+}
+
 template <class V>
 __device__ __forceinline__ V cgroup_sum(unsigned peers, V val, bool leader) {
     int maxsize = __reduce_max_sync(FULL, (unsigned)__popc(peers));
@@ -120,25 +201,29 @@ __device__ __forceinline__ V cgroup_sum(unsigned peers, V val, bool leader) {
     return s;
 }
 
-// one 32-edge chunk of coarse vertex c's flat list: q = base + lane
+// one 32-entry chunk of a coarse row's flat list: q = base + lane; the
+// warp pre-aggregates equal keys with __match_any_sync before the table insert
 template <class W>
-__device__ __forceinline__ void cchunk(const CArgs<W>& a, i32 c, i64 m0, i64 m1, i64 q, i64 qend, i32* keys,
-                                       typename Traits<W>::V* vals, u32 mask) {
+__device__ __forceinline__ typename Traits<W>::V cchunk_load(const CArgs<W>& a, i64 q, i64 qend, i32& key,
+                                                             bool& keep, bool& leader) {
     using V = typename Traits<W>::V;
-    bool valid = q < qend;
-    i32 u = -1;
-    V wv = V(0);
-    if (valid) {
-        i64 j = flat_edge(a.P, a.members, a.g.rowptr, m0, m1, q);
-        u = a.vcmap[a.g.col[j]];
-        wv = V(a.g.wgt(j));
-    }
-    bool keep = valid && u != c;
-    i32 key = keep ? u : (i32)(0x80000000u | lane_id());
-    unsigned peers = __match_any_sync(FULL, key);
-    bool leader = keep && ((peers & lanemask_lt()) == 0);
-    V s = a.g.w ? cgroup_sum<V>(peers, wv, leader) : V(__popc(peers));
-    if (leader) ctable_add(keys, vals, mask, u, s, a.err, a.probe_cap);
+    const bool valid = q < qend;
+    const i32 u = valid ? a.fkey[q] : -1;
+    const V wv = (valid && a.g.w) ? V(a.fw[q]) : V(0);
+    keep = valid && u >= 0;
+    key = keep ? u : (i32)(0x80000000u | lane_id());
+    const unsigned peers = __match_any_sync(FULL, key);
+    leader = keep && ((peers & lanemask_lt()) == 0);
+    return a.g.w ? cgroup_sum<V>(peers, wv, leader) : V(__popc(peers));
+}
+
+template <class W>
+__device__ __forceinline__ void cchunk(const CArgs<W>& a, i64 q, i64 qend, i32* keys, typename Traits<W>::V* vals,
+                                       u32 mask) {
+    i32 key;
+    bool keep, leader;
+    auto s = cchunk_load(a, q, qend, key, keep, leader);
+    if (leader) ctable_add(keys, vals, mask, key, s, a.err, a.probe_cap);
 }
 
 // warp per coarse row with a per-warp shared-memory table of CW_T slots
@@ -165,7 +250,7 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_contract_warp(CArgs<W> a, con
             vals[s] = V(0);
         }
         __syncwarp();
-        for (i64 q = q0 + l; q - l < q1; q += 32) cchunk(a, c, m0, m1, q, q1, keys, vals, T - 1);
+        for (i64 q = q0 + l; q - l < q1; q += 32) cchunk(a, q, q1, keys, vals, T - 1);
         __syncwarp();
         i64 written = 0;
         for (u32 s0 = 0; s0 < T; s0 += 32) {
@@ -185,13 +270,17 @@ __global__ void __launch_bounds__(CW_WARPS * 32) k_contract_warp(CArgs<W> a, con
 }
 
 // block per coarse row; the table is in shared memory (`gcap` slots, sized to
-// the bucket's largest table) or, with GLOBAL, in a per-block global region
-template <class W, bool GLOBAL>
-__global__ void __launch_bounds__(256) k_contract_block(CArgs<W> a, const i32* list, const i64* d_count, i32* gkeys,
-                                                        typename Traits<W>::V* gvals, i64 gcap, i64 nc) {
+// the bucket's largest table) or, with GLOBAL, in a per-block global region.
+// With OVF (shared tables of gcap slots smaller than 2U), a row whose distinct
+// keys do not fit is appended to `ovf_list` for the global-table pass instead.
+template <class W, bool GLOBAL, int THREADS = 256, bool OVF = false>
+__global__ void __launch_bounds__(THREADS) k_contract_block(CArgs<W> a, const i32* list, const i64* d_count, i32* gkeys,
+                                                            typename Traits<W>::V* gvals, i64 gcap, i64 nc,
+                                                            i32* ovf_list = nullptr, i64* ovf_count = nullptr) {
     using V = typename Traits<W>::V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long wcount;
+    __shared__ int full;
     V* svals = (V*)smem_raw;
     i32* skeys = (i32*)(smem_raw + sizeof(V) * (GLOBAL ? 0 : gcap));
     const int l = lane_id(), w = threadIdx.x >> 5;
@@ -204,15 +293,38 @@ __global__ void __launch_bounds__(256) k_contract_block(CArgs<W> a, const i32* l
         i64 q0 = a.P[m0], q1 = a.P[m1];
         i64 U = min(q1 - q0, nc);
         u32 T = next_pow2_u32((u32)(2 * (U > 1 ? U : 1)));
-        for (u32 s = threadIdx.x; s < T; s += 256) {
+        if (OVF && T > (u32)gcap) T = (u32)gcap;
+        for (u32 s = threadIdx.x; s < T; s += THREADS) {
             keys[s] = -1;
             vals[s] = V(0);
         }
-        if (threadIdx.x == 0) wcount = 0;
+        if (threadIdx.x == 0) {
+            wcount = 0;
+            full = 0;
+        }
         __syncthreads();
-        for (i64 q = q0 + (i64)w * 32 + l; q - l < q1; q += 256) cchunk(a, c, m0, m1, q, q1, keys, vals, T - 1);
+        if (OVF) {
+            for (i64 q = q0 + (i64)w * 32 + l; q - l < q1; q += THREADS) {
+                i32 key;
+                bool keep, leader;
+                auto sv = cchunk_load(a, q, q1, key, keep, leader);
+                if (leader && !ctable_try_add(keys, vals, T - 1, key, sv)) full = 1;
+                if (__any_sync(FULL, *(volatile int*)&full != 0)) break;
+            }
+            __syncthreads();
+            if (full) {
+                if (threadIdx.x == 0) {
+                    i64 k = (i64)::atomicAdd((unsigned long long*)ovf_count, 1ull);
+                    ovf_list[k] = c;
+                }
+                __syncthreads();
+                continue;
+            }
+        } else {
+            for (i64 q = q0 + (i64)w * 32 + l; q - l < q1; q += THREADS) cchunk(a, q, q1, keys, vals, T - 1);
+        }
         __syncthreads();
-        for (u32 s0 = w * 32; s0 < T; s0 += 256) {
+        for (u32 s0 = w * 32; s0 < T; s0 += THREADS) {
             u32 s = s0 + l;
             bool occ = s < T && keys[s] != -1;
             unsigned m = __ballot_sync(FULL, occ);
@@ -372,45 +484,69 @@ __global__ void k_big_place(const i32* list, i64 count, const i64* tstart, const
     }
 }
 
-__global__ void k_max_bound(const i32* list, const i64* d_count, const i64* P, const i64* cstart,
-                            unsigned long long* out) {
-    const i64 count = *d_count;
-    unsigned long long m = 0;
-    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < count; x += (i64)gridDim.x * blockDim.x) {
-        i32 c = list[x];
-        unsigned long long b = (unsigned long long)(P[cstart[c + 1]] - P[cstart[c]]);
-        m = b > m ? b : m;
+// Sorts the coarse rows into the hashing buckets in one pass (list order is
+// irrelevant: rows are independent).  Buckets by bound (sum of member degrees)
+// and U = min(bound, nc): 0: bound <= 32, 1: bound <= 256, 2: U <= 1024,
+// 3: U <= 4096, 4: above.  cnt[k] counts bucket k; cnt[5] is the largest
+// bound of bucket 4.
+__global__ void k_bucket_rows(const i64* P, const i64* cstart, i64 nc, i32* l0, i32* l1, i32* l2, i32* l3, i32* l4,
+                              unsigned long long* cnt) {
+    const int l = lane_id();
+    unsigned long long mx = 0;
+    for (i64 c0 = (blockIdx.x * (i64)blockDim.x + threadIdx.x) - l; c0 < nc; c0 += (i64)gridDim.x * blockDim.x) {
+        const i64 c = c0 + l;
+        int k = -1;
+        if (c < nc) {
+            const i64 v = P[cstart[c + 1]] - P[cstart[c]];
+            const i64 U = v < nc ? v : nc;
+            k = v <= 32 ? 0 : v <= 256 ? 1 : U <= 1024 ? 2 : U <= HUGE_DEG ? 3 : 4;
+            if (k == 4 && (unsigned long long)v > mx) mx = (unsigned long long)v;
+        }
+        i32* lists[5] = {l0, l1, l2, l3, l4};
+#pragma unroll
+        for (int b = 0; b < 5; b++) {
+            const unsigned m = __ballot_sync(FULL, k == b);
+            if (!m) continue;
+            const int leader = __ffs(m) - 1;
+            unsigned long long base = 0;
+            if (l == leader) base = atomicAdd(&cnt[b], (unsigned long long)__popc(m));
+            base = __shfl_sync(FULL, base, leader);
+            if (k == b) lists[b][base + __popc(m & lanemask_lt())] = (i32)c;
+        }
     }
     for (int d = 16; d >= 1; d >>= 1) {
-        unsigned long long o = __shfl_xor_sync(FULL, m, d);
-        m = o > m ? o : m;
+        const unsigned long long o = __shfl_xor_sync(FULL, mx, d);
+        mx = o > mx ? o : mx;
     }
-    if (lane_id() == 0 && m) atomicMax(out, m);
+    if (l == 0 && mx) atomicMax(&cnt[5], mx);
 }
 
-struct BucketFlag {
-    const i64* val;
-    i64 lo, hi;  // lo < v <= hi
-    __device__ i64 operator()(i64 c) const {
-        i64 v = val[c];
-        return (v > lo && v <= hi) ? 1 : 0;
+// Placement buckets by unique count u: 0: u <= 32, 1: u <= PW_MAX,
+// 2: u <= PB_MAX, 3: above (rows with no entries are skipped).
+__global__ void k_bucket_place(const i64* ucount, i64 nc, i32* l0, i32* l1, i32* l2, i32* l3,
+                               unsigned long long* cnt) {
+    const int l = lane_id();
+    for (i64 c0 = (blockIdx.x * (i64)blockDim.x + threadIdx.x) - l; c0 < nc; c0 += (i64)gridDim.x * blockDim.x) {
+        const i64 c = c0 + l;
+        int k = -1;
+        if (c < nc) {
+            const i64 u = ucount[c];
+            k = u <= 0 ? -1 : u <= 32 ? 0 : u <= PW_MAX ? 1 : u <= PB_MAX ? 2 : 3;
+        }
+        i32* lists[4] = {l0, l1, l2, l3};
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const unsigned m = __ballot_sync(FULL, k == b);
+            if (!m) continue;
+            const int leader = __ffs(m) - 1;
+            unsigned long long base = 0;
+            if (l == leader) base = atomicAdd(&cnt[b], (unsigned long long)__popc(m));
+            base = __shfl_sync(FULL, base, leader);
+            if (k == b) lists[b][base + __popc(m & lanemask_lt())] = (i32)c;
+        }
     }
-};
-// lo < bound <= hi, and for mode 1 / 2 also U = min(bound, nc) <= / > 4096
-struct BoundFlag {
-    const i64* P;
-    const i64* cstart;
-    i64 lo, hi, nc;
-    int mode;
-    __device__ i64 operator()(i64 c) const {
-        i64 v = P[cstart[c + 1]] - P[cstart[c]];
-        if (!(v > lo && v <= hi)) return 0;
-        i64 U = v < nc ? v : nc;
-        if (mode == 1) return U <= HUGE_DEG ? 1 : 0;
-        if (mode == 2) return U > HUGE_DEG ? 1 : 0;
-        return 1;
-    }
-};
+}
+
 struct IdxEpiC {
     i32* dst;
     __device__ void operator()(i64 x, i64 excl, i64 v) const {
@@ -453,6 +589,7 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     }
     DBuf<i64> cnt(ctx, nc + 1), bound(ctx, nc + 1), cstart(ctx, nc + 1), P(ctx, n + 1), ucount(ctx, nc + 1);
     DBuf<i32> members(ctx, n);
+    DBuf<i64> memberpos(ctx, n);
     PGGC_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(i64) * (nc + 1), ctx.stream));
     PGGC_CUDA(cudaMemsetAsync(bound.p, 0, sizeof(i64) * (nc + 1), ctx.stream));
     int gridv = (int)std::min<i64>(ceil_div(n, 256), (i64)ctx.num_sms * 16);
@@ -462,32 +599,45 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     {
         DBuf<i64> cursor(ctx, nc + 1);
         copy_d2d(ctx, cursor.p, cstart.p, nc + 1);
-        k_scatter_members<<<gridv, 256, 0, ctx.stream>>>(vcmap, n, cursor.p, members.p);
+        k_scatter_members<<<gridv, 256, 0, ctx.stream>>>(vcmap, n, cursor.p, members.p, memberpos.p);
         PGGC_LAUNCH_CHECK();
     }
     DBuf<i64> tot(ctx, 4);
     scan_apply(ctx, MemberDegIn{gv.rowptr, members.p, n}, ArrOutExcl{P.p}, n + 1, nullptr, tot.p);
+    // flattened rows: coarse key and weight of every fine edge at its flat position
+    DBuf<i32> fkey(ctx, std::max<i64>(g.nnz, 1));
+    DBuf<W> fw;
+    if (gv.w) fw = DBuf<W>(ctx, std::max<i64>(g.nnz, 1));
+    if (g.nnz > 0) {
+        int grid = (int)std::min<i64>(ceil_div(ceil_div(n, 32), 8), (i64)ctx.num_sms * 16);
+        k_flatten<W><<<grid, 256, 0, ctx.stream>>>(gv, vcmap, P.p, memberpos.p, fkey.p, fw.p);
+        PGGC_LAUNCH_CHECK();
+    }
     const i64 total_bound = g.nnz;
     DBuf<i32> okey(ctx, std::max<i64>(total_bound, 1));
     DBuf<V> oval(ctx, std::max<i64>(total_bound, 1));
 
-    // bucket lists by table size U = min(bound, nc) and bound:
-    //   small warp rows (bound <= 32), medium warp rows (bound <= 256),
-    //   block rows with a shared-memory table (U <= 4096), global-table rows
-    DBuf<i32> lw(ctx, nc), lm(ctx, nc), lb(ctx, nc), lh(ctx, nc);
-    DBuf<i64> counts(ctx, 12);
-    PGGC_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(i64) * 12, ctx.stream));
-    scan_apply(ctx, BoundFlag{P.p, cstart.p, -1, 32, nc, 0}, IdxEpiC{lw.p}, nc, nullptr, counts.p + 0);
-    scan_apply(ctx, BoundFlag{P.p, cstart.p, 32, 256, nc, 0}, IdxEpiC{lm.p}, nc, nullptr, counts.p + 8);
-    scan_apply(ctx, BoundFlag{P.p, cstart.p, 256, (i64)1 << 62, nc, 1}, IdxEpiC{lb.p}, nc, nullptr, counts.p + 1);
-    scan_apply(ctx, BoundFlag{P.p, cstart.p, 256, (i64)1 << 62, nc, 2}, IdxEpiC{lh.p}, nc, nullptr, counts.p + 2);
-    k_max_bound<<<64, 256, 0, ctx.stream>>>(lh.p, counts.p + 2, P.p, cstart.p, (unsigned long long*)(counts.p + 7));
-    PGGC_LAUNCH_CHECK();
-    k_max_bound<<<64, 256, 0, ctx.stream>>>(lb.p, counts.p + 1, P.p, cstart.p, (unsigned long long*)(counts.p + 9));
-    PGGC_LAUNCH_CHECK();
-    // one round trip: bucket sizes and the largest bounds
-    const i64* hc = (const i64*)ctx.readback(counts.p, 12 * sizeof(i64));
-    const i64 n_w = hc[0], n_b = hc[1], n_h = hc[2], max_huge = hc[7], n_m = hc[8], max_block = hc[9];
+    // bucket lists by bound (sum of member degrees) and table size U =
+    // min(bound, nc): small warp rows (bound <= 32), medium warp rows
+    // (bound <= 256), block rows with shared tables of 2048 slots (U <= 1024)
+    // and 8192 slots (U <= 4096), big rows with 16384-slot shared tables
+    // (U > 4096) whose overflow falls back to global tables
+    DBuf<i32> lw(ctx, nc), lm(ctx, nc), lb(ctx, nc), lb2(ctx, nc), lh(ctx, nc), lo(ctx, nc);
+    // counts: [0] small warp rows, [1] medium warp rows, [2] 2048-slot block
+    // rows, [3] 8192-slot block rows, [4] big rows, [5] largest big-row bound,
+    // [6] overflow rows, [7..10] placement buckets, [11] coarse nnz,
+    // [12] big-row placement total
+    DBuf<i64> counts(ctx, 16);
+    PGGC_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(i64) * 16, ctx.stream));
+    {
+        int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(nc, 256), (i64)ctx.num_sms * 8));
+        k_bucket_rows<<<grid, 256, 0, ctx.stream>>>(P.p, cstart.p, nc, lw.p, lm.p, lb.p, lb2.p, lh.p,
+                                                   (unsigned long long*)counts.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    // one round trip: bucket sizes and the largest big-row bound
+    const i64* hc = (const i64*)ctx.readback(counts.p, 16 * sizeof(i64));
+    const i64 n_w = hc[0], n_m = hc[1], n_b = hc[2], n_b2 = hc[3], n_h = hc[4], max_huge = hc[5];
 
     CArgs<W> a;
     a.g = gv;
@@ -495,6 +645,8 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     a.cstart = cstart.p;
     a.members = members.p;
     a.P = P.p;
+    a.fkey = fkey.p;
+    a.fw = fw.p;
     a.out_key = okey.p;
     a.out_val = oval.p;
     a.ucount = ucount.p;
@@ -509,64 +661,79 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     if (n_m > 0) {
         constexpr int WARPS = 4;
         int grid = (int)std::min<i64>(ceil_div(n_m, WARPS), (i64)ctx.num_sms * 16);
-        k_contract_warp<W, 512, WARPS><<<grid, WARPS * 32, 0, ctx.stream>>>(a, lm.p, counts.p + 8);
+        k_contract_warp<W, 512, WARPS><<<grid, WARPS * 32, 0, ctx.stream>>>(a, lm.p, counts.p + 1);
         PGGC_LAUNCH_CHECK();
     }
+    const size_t slot = sizeof(V) + sizeof(i32);
     if (n_b > 0) {
-        // table sized to the largest row of the bucket
-        i64 tmax = next_pow2_u32((u32)(2 * std::max<i64>(std::min<i64>(max_block, nc), 1)));
-        size_t sm = (sizeof(V) + sizeof(i32)) * (size_t)tmax;
-        set_dynamic_smem_once(k_contract_block<W, false>, (int)((sizeof(V) + sizeof(i32)) * SEL_TS_MAX), ctx.device);
-        int per_sm = 0;
-        PGGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_block<W, false>, 256, sm));
-        int grid = (int)std::min<i64>(n_b, (i64)ctx.num_sms * std::max(per_sm, 1));
-        k_contract_block<W, false><<<grid, 256, sm, ctx.stream>>>(a, lb.p, counts.p + 1, nullptr, nullptr, tmax, nc);
+        constexpr int TS = 2048;
+        int grid = (int)std::min<i64>(n_b, (i64)ctx.num_sms * 8);
+        k_contract_block<W, false, 256><<<grid, 256, slot * TS, ctx.stream>>>(a, lb.p, counts.p + 2, nullptr, nullptr,
+                                                                               TS, nc);
+        PGGC_LAUNCH_CHECK();
+    }
+    if (n_b2 > 0) {
+        constexpr int TS = 2 * HUGE_DEG;
+        set_dynamic_smem_once(k_contract_block<W, false, 512>, (int)(slot * TS), ctx.device);
+        int grid = (int)std::min<i64>(n_b2, (i64)ctx.num_sms * 2);
+        k_contract_block<W, false, 512><<<grid, 512, slot * TS, ctx.stream>>>(a, lb2.p, counts.p + 3, nullptr, nullptr,
+                                                                               TS, nc);
         PGGC_LAUNCH_CHECK();
     }
     if (n_h > 0) {
-        // global tables sized for the largest table among the huge rows, one
-        // region per resident block, at most 2 GiB of tables
+        // 16384-slot shared tables; rows with more distinct neighbours (a
+        // 64-probe insert failure) go to the overflow list
+        constexpr int TS = 16384;
+        set_dynamic_smem_once(k_contract_block<W, false, 1024, true>, (int)(slot * TS), ctx.device);
+        int grid = (int)std::min<i64>(n_h, (i64)ctx.num_sms);
+        k_contract_block<W, false, 1024, true><<<grid, 1024, slot * TS, ctx.stream>>>(
+            a, lh.p, counts.p + 4, nullptr, nullptr, TS, nc, lo.p, counts.p + 6);
+        PGGC_LAUNCH_CHECK();
+        // global tables sized for the largest table among the big rows, one
+        // region per resident block, at most 2 GiB of tables; the blocks
+        // beyond the overflow count exit at once
         i64 maxb = std::min<i64>(max_huge, nc);
         i64 gcap = next_pow2_u32((u32)std::min<i64>(2 * std::max<i64>(maxb, 1), (i64)1 << 30));
-        i64 by_mem = std::max<i64>(1, ((i64)2 << 30) / (gcap * (i64)(sizeof(V) + sizeof(i32))));
-        int grid = (int)std::min<i64>(std::min<i64>(n_h, (i64)ctx.num_sms * 2), by_mem);
-        i32* gk = ctx.ws_get<i32>(WS_CONTRACT_GK, gcap * grid);
-        V* gvv = ctx.ws_get<V>(WS_CONTRACT_GV, gcap * grid);
-        k_contract_block<W, true><<<grid, 256, 0, ctx.stream>>>(a, lh.p, counts.p + 2, gk, gvv, gcap, nc);
+        i64 by_mem = std::max<i64>(1, ((i64)2 << 30) / (gcap * (i64)slot));
+        int ggrid = (int)std::min<i64>(std::min<i64>(n_h, (i64)ctx.num_sms * 2), by_mem);
+        i32* gk = ctx.ws_get<i32>(WS_CONTRACT_GK, gcap * ggrid);
+        V* gvv = ctx.ws_get<V>(WS_CONTRACT_GV, gcap * ggrid);
+        k_contract_block<W, true><<<ggrid, 256, 0, ctx.stream>>>(a, lo.p, counts.p + 6, gk, gvv, gcap, nc);
         PGGC_LAUNCH_CHECK();
     }
     // coarse row offsets, placement buckets and the big-row total, then one round trip
-    scan_apply(ctx, UcountIn{ucount.p, nc}, RowptrOut{cg->rowptr.p}, nc + 1, nullptr, tot.p + 1);
+    scan_apply(ctx, UcountIn{ucount.p, nc}, RowptrOut{cg->rowptr.p}, nc + 1, nullptr, counts.p + 11);
     DBuf<i32> pw(ctx, nc), pr(ctx, nc), pb(ctx, nc), ph(ctx, nc);
-    scan_apply(ctx, BucketFlag{ucount.p, 0, 32}, IdxEpiC{pw.p}, nc, nullptr, counts.p + 3);
-    scan_apply(ctx, BucketFlag{ucount.p, 32, PW_MAX}, IdxEpiC{pr.p}, nc, nullptr, counts.p + 10);
-    scan_apply(ctx, BucketFlag{ucount.p, PW_MAX, PB_MAX}, IdxEpiC{pb.p}, nc, nullptr, counts.p + 4);
-    scan_apply(ctx, BucketFlag{ucount.p, PB_MAX, (i64)1 << 62}, IdxEpiC{ph.p}, nc, nullptr, counts.p + 5);
+    {
+        int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(nc, 256), (i64)ctx.num_sms * 8));
+        k_bucket_place<<<grid, 256, 0, ctx.stream>>>(ucount.p, nc, pw.p, pr.p, pb.p, ph.p,
+                                                    (unsigned long long*)(counts.p + 7));
+        PGGC_LAUNCH_CHECK();
+    }
     DBuf<i64> tstart(ctx, nc + 1);
-    scan_apply(ctx, ListUIn{ph.p, ucount.p, counts.p + 5}, ArrOutExcl{tstart.p}, nc + 1, nullptr, tot.p + 2);
-    PGGC_CUDA(cudaMemcpyAsync(counts.p + 6, tot.p + 1, 2 * sizeof(i64), cudaMemcpyDeviceToDevice, ctx.stream));
-    const i64* pc = (const i64*)ctx.readback(counts.p, 12 * sizeof(i64));
-    const i64 p_w = pc[3], p_b = pc[4], p_h = pc[5], nnz_c = pc[6], tn = pc[7], p_r = pc[10];
+    scan_apply(ctx, ListUIn{ph.p, ucount.p, counts.p + 10}, ArrOutExcl{tstart.p}, nc + 1, nullptr, counts.p + 12);
+    const i64* pc = (const i64*)ctx.readback(counts.p, 16 * sizeof(i64));
+    const i64 p_w = pc[7], p_r = pc[8], p_b = pc[9], p_h = pc[10], nnz_c = pc[11], tn = pc[12];
     ctx.check_device_error();
     cg->nnz = nnz_c;
     cg->col = DBuf<i32>(ctx, std::max<i64>(nnz_c, 1));
     cg->w = DBuf<W>(ctx, std::max<i64>(nnz_c, 1));
     if (p_w > 0) {
         int grid = (int)std::min<i64>(ceil_div(p_w, 8), (i64)ctx.num_sms * 8);
-        k_place_warp<W><<<grid, 256, 0, ctx.stream>>>(pw.p, counts.p + 3, P.p, cstart.p, ucount.p, cg->rowptr.p, okey.p,
+        k_place_warp<W><<<grid, 256, 0, ctx.stream>>>(pw.p, counts.p + 7, P.p, cstart.p, ucount.p, cg->rowptr.p, okey.p,
                                                       oval.p, cg->col.p, cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
     if (p_r > 0) {
         int grid = (int)std::min<i64>(ceil_div(p_r, PW_WARPS), (i64)ctx.num_sms * 8);
-        k_place_warp_rank<W><<<grid, PW_WARPS * 32, 0, ctx.stream>>>(pr.p, counts.p + 10, P.p, cstart.p, ucount.p,
+        k_place_warp_rank<W><<<grid, PW_WARPS * 32, 0, ctx.stream>>>(pr.p, counts.p + 8, P.p, cstart.p, ucount.p,
                                                                      cg->rowptr.p, okey.p, oval.p, cg->col.p,
                                                                      cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
     if (p_b > 0) {
         int grid = (int)std::min<i64>(p_b, (i64)ctx.num_sms * 4);
-        k_place_block<W><<<grid, 256, 0, ctx.stream>>>(pb.p, counts.p + 4, P.p, cstart.p, ucount.p, cg->rowptr.p,
+        k_place_block<W><<<grid, 256, 0, ctx.stream>>>(pb.p, counts.p + 9, P.p, cstart.p, ucount.p, cg->rowptr.p,
                                                        okey.p, oval.p, cg->col.p, cg->w.p);
         PGGC_LAUNCH_CHECK();
     }

@@ -7,6 +7,7 @@
 // coarse maps) and sequences the kernel families.  Decisions the reference
 // makes on host scalars (objective unchanged, label_count == n, coarse count)
 // stay on the host; everything else stays on the device.
+#include <limits>
 #include "kernels.cuh"
 
 namespace pggc {
@@ -352,7 +353,52 @@ void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Trait
     }
 }
 
+// run_clustering (app/cluster_main.cpp:116-165): the method, then improvement
+// passes while iteration_termination_condition (:101-114) says continue
+template <class W>
+void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Traits<W>::V>& cs, int method, int ex_iters,
+                    u64 seed, i32* labels_out, RunStats* rs) {
+    const i64 n = g.n;
+    DBuf<i32> part(ctx, std::max<i64>(n, 1)), con(ctx, std::max<i64>(n, 1));
+    RunStats acc;
+    u64 pass = 0;
+    auto one = [&](bool improve) {
+        RunStats r1;
+        if (method == METHOD_LOUVAIN) {
+            louvain_part<W>(ctx, g, cs, improve, con.p, part.p, &r1);
+        } else {
+            u64 s = seed + 0x9E3779B97F4A7C15ull * pass;
+            pass++;
+            leiden_part<W>(ctx, g, cs, method == METHOD_LEIDEN_PLUS, improve, con.p, s, part.p, &r1);
+        }
+        acc.levels = r1.levels;
+        acc.total_nnz = r1.total_nnz;
+        acc.sweeps += r1.sweeps;
+        acc.moves += r1.moves;
+        acc.passes++;
+    };
+    one(false);
+    double last = -std::numeric_limits<double>::infinity();
+    int counter = 0;
+    while (true) {
+        bool terminate = true;
+        if (ex_iters < 0) {
+            if (cs.get_objective() > last) terminate = false;
+            last = cs.get_objective();
+        } else {
+            if (counter++ < ex_iters) terminate = false;
+        }
+        if (terminate) break;
+        copy_d2d(ctx, con.p, part.p, n);
+        one(true);
+    }
+    copy_d2d(ctx, labels_out, part.p, n);
+    if (rs) *rs = acc;
+}
+
 #define PGGC_INST_DRV(W)                                                                                              \
+    template void run_clustering<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, int, int, u64, i32*,      \
+                                    RunStats*);                                                                       \
     template void leiden_part<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, bool, bool, const i32*, u64, \
                                  i32*, RunStats*);                                                                    \
     template void louvain_part<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, bool, const i32*, i32*,     \

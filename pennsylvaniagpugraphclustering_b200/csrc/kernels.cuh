@@ -138,9 +138,15 @@ struct RunStats {
     i64 passes = 0;
 };
 
+enum Method { METHOD_LOUVAIN = 0, METHOD_LEIDEN = 1, METHOD_LEIDEN_PLUS = 2 };
+
 template <class W>
 void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool plus, bool improve,
                  const i32* input, u64 seed, i32* labels_out, RunStats* st);
+// the method then ex_iters improvement passes (< 0: while the objective rises)
+template <class W>
+void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Traits<W>::V>& cs, int method, int ex_iters,
+                    u64 seed, i32* labels_out, RunStats* rs);
 template <class W>
 void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool constrained,
                   const i32* constraint, i32* labels_out, RunStats* st);

@@ -279,13 +279,16 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, R
     if (a.prof && l == 0 && pb) atomicAdd(a.prof, pb);
 }
 
-// ---- degree classes for sub-warp groups ------------------------------------
-// The vertices of order1 bucket 0 (degree < 128) are split by degree into
-// class 0 (<= 8), 1 (<= 16), 2 (<= 32) and 3 (< 128) so that a warp can serve
-// 4, 2 or 1 low-degree vertices at once.  Order inside a class is irrelevant:
-// every consumer treats vertices independently.
-constexpr int NCLS = 4;
-__device__ __forceinline__ int deg_class(i64 d) { return d <= 8 ? 0 : (d <= 16 ? 1 : (d <= 32 ? 2 : 3)); }
+// ---- degree classes ---------------------------------------------------------
+// All vertices are split by degree into class 0 (<= 8), 1 (<= 16), 2 (<= 32),
+// 3 (< 128: order1 bucket 0), 4 (<= 1024), 5 (<= 4096) and 6 (above), so that
+// a warp can serve 4, 2 or 1 low-degree vertices at once and the block
+// kernels get shared tables sized to their class (2048 or 8192 slots).  Order
+// inside a class is irrelevant: every consumer treats vertices independently.
+constexpr int NCLS = 7;
+__device__ __forceinline__ int deg_class(i64 d) {
+    return d <= 8 ? 0 : d <= 16 ? 1 : d <= 32 ? 2 : d < LARGE_CUTOFF ? 3 : d <= 1024 ? 4 : d <= HUGE_DEG ? 5 : 6;
+}
 
 struct ClassLists {
     i32* list = nullptr;          // [count] vertices grouped by class
@@ -343,10 +346,10 @@ __global__ void k_class_scatter(const i32* list, i64 count, const i64* rowptr, u
     }
 }
 
-// Builds the class lists of order1[0, off_large) into workspace slots.
+// Builds the class lists of all vertices into workspace slots.
 inline void build_class_lists(Context& ctx, const i64* rowptr, const Ordering& ord, int slot_list, int slot_off,
                               int slot_cnt, ClassLists& cl) {
-    cl.count = ord.off_large;
+    cl.count = ord.n;
     cl.list = ctx.ws_get<i32>(slot_list, std::max<i64>(cl.count, 1));
     cl.off = ctx.ws_get<i64>(slot_off, NCLS + 1);
     cl.cnt = ctx.ws_get<unsigned long long>(slot_cnt, 2 * NCLS);
@@ -425,21 +428,23 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
     }
 }
 
-// ---- block per vertex (256 threads), shared or global table ----------------
-template <class W, bool CON, bool GLOBAL>
-__global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* list, i64 count, i32* gkeys,
-                                                      typename Traits<W>::V* gvals, i64 gcap) {
+// ---- block per vertex, shared or global table -------------------------------
+template <class W, bool CON, bool GLOBAL, int THREADS = 256>
+__global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg, i32* gkeys,
+                                                          typename Traits<W>::V* gvals, i64 gcap) {
     using V = typename Traits<W>::V;
+    constexpr int NW = THREADS / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ Best wb[8];
+    __shared__ Best wb[NW];
     V* svals = (V*)smem_raw;
     i32* skeys = (i32*)(smem_raw + sizeof(V) * (GLOBAL ? 0 : gcap));  // gcap = shared table slots
     const int l = lane_id(), w = threadIdx.x >> 5;
     i32* keys = GLOBAL ? gkeys + (i64)blockIdx.x * gcap : skeys;
     V* vals = GLOBAL ? gvals + (i64)blockIdx.x * gcap : svals;
     unsigned long long pb = 0;
-    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
-        i32 i = list[x];
+    const i64 lo = rg.begin(), count = rg.end();
+    for (i64 x = lo + blockIdx.x; x < count; x += gridDim.x) {
+        i32 i = rg.list[x];
         i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
         if (!GLOBAL && e - b > HUGE_DEG) continue;
         if (a.dest[i] == NO_MOVE) {
@@ -450,18 +455,19 @@ __global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* l
         VCtx vc = sel_prologue(a, i);
         Best best = none_best();
         if (a.initial) {
-            for (i64 j = b + threadIdx.x; j < e; j += 256) sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
+            for (i64 j = b + threadIdx.x; j < e; j += THREADS)
+                sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
         } else {
             i64 U = min(e - b, *a.label_count);
             u32 T = next_pow2_u32((u32)(2 * U));
-            for (u32 s = threadIdx.x; s < T; s += 256) {
+            for (u32 s = threadIdx.x; s < T; s += THREADS) {
                 keys[s] = -1;
                 vals[s] = V(0);
             }
             __syncthreads();
-            for (i64 j = b + (i64)w * 32 + l; j - l < e; j += 256) chunk_to_table(a, vc, j, e, keys, vals, T - 1);
+            for (i64 j = b + (i64)w * 32 + l; j - l < e; j += THREADS) chunk_to_table(a, vc, j, e, keys, vals, T - 1);
             __syncthreads();
-            for (u32 s = threadIdx.x; s < T; s += 256) {
+            for (u32 s = threadIdx.x; s < T; s += THREADS) {
                 i32 c = keys[s];
                 if (c != -1) sel_eval<W, CON>(a, vc, c, vals[s], best);
             }
@@ -470,7 +476,7 @@ __global__ void __launch_bounds__(256) k_select_block(SelArgs<W> a, const i32* l
         if (l == 0) wb[w] = best;
         __syncthreads();
         if (w == 0) {
-            best = l < 8 ? wb[l] : none_best();
+            best = l < NW ? wb[l] : none_best();
             warp_best(best);
             if (l == 0) sel_finish(a, i, vc, best);
         }
@@ -1300,25 +1306,26 @@ struct Mover {
         if (nb > 0) {
             ProfScope ps(ctx, "select_block");
             a.prof = ctx.prof_counter("select_block");
-            // shared table sized to the largest table a vertex of this bucket can need
-            i64 umax = std::max<i64>(1, std::min<i64>(std::min<i64>(ord.max_deg, HUGE_DEG),
-                                                      label_bound_host > 0 ? label_bound_host : HUGE_DEG));
-            i64 tmax = next_pow2_u32((u32)(2 * umax));
-            size_t sm = (sizeof(V) + sizeof(i32)) * (size_t)tmax;
-            set_dynamic_smem_once(k_select_block<W, CON, false>, (int)((sizeof(V) + sizeof(i32)) * SEL_TS_MAX),
-                                  ctx.device);
-            int per_sm = 0;
-            PGGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_select_block<W, CON, false>, 256, sm));
-            int grid = (int)std::min<i64>(nb, (i64)ctx.num_sms * std::max(per_sm, 1));
-            k_select_block<W, CON, false><<<grid, 256, sm, ctx.stream>>>(a, ord.order1.p + ord.off_large, nb, nullptr,
-                                                                         nullptr, tmax);
+            // class 4 (degree <= 1024): 2048-slot tables, 8 blocks of 256 per SM;
+            // class 5 (degree <= 4096): 8192-slot tables, 2 blocks of 512 per SM
+            const size_t slot = sizeof(V) + sizeof(i32);
+            const i64 n4 = std::min<i64>(nb, (i64)ctx.num_sms * 8), n5 = std::min<i64>(nb, (i64)ctx.num_sms * 2);
+            k_select_block<W, CON, false, 256><<<(int)n4, 256, slot * 2048, ctx.stream>>>(
+                a, dev_range(cls.list, cls.off + 4, cls.off + 5), nullptr, nullptr, 2048);
             PGGC_LAUNCH_CHECK();
+            if (ord.max_deg > 1024) {
+                set_dynamic_smem_once(k_select_block<W, CON, false, 512>, (int)(slot * SEL_TS_MAX), ctx.device);
+                k_select_block<W, CON, false, 512><<<(int)n5, 512, slot * SEL_TS_MAX, ctx.stream>>>(
+                    a, dev_range(cls.list, cls.off + 5, cls.off + 6), nullptr, nullptr, SEL_TS_MAX);
+                PGGC_LAUNCH_CHECK();
+            }
         }
         if (ord.n_huge > 0) {
             ProfScope ps(ctx, "select_huge");
             a.prof = ctx.prof_counter("select_huge");
             int grid = (int)std::min<i64>(ord.n_huge, 32);
-            k_select_block<W, CON, true><<<grid, 256, 0, ctx.stream>>>(a, ord.huge.p, ord.n_huge, gkeys.p, gvals.p, gcap);
+            k_select_block<W, CON, true><<<grid, 256, 0, ctx.stream>>>(a, host_range(ord.huge.p, 0, ord.n_huge), gkeys.p,
+                                                                       gvals.p, gcap);
             PGGC_LAUNCH_CHECK();
         }
     }

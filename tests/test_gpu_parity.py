@@ -245,3 +245,23 @@ def test_verify_objective(mem, name):
     vo, ro = O.verify_objective(og, labels, obj)
     vg, rg = pg.verify_objective(mem, wg, labels, obj)
     assert vo == vg and ro == rg
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_build_coarse_graph_row_wider_than_shared_table(mem, weighted):
+    """A coarse row with ~40,000 distinct neighbours: more than a 16,384-slot
+    shared table holds, so the row takes the global-table fallback."""
+    leaves = 40000
+    rng = np.random.default_rng(4)
+    w = rng.uniform(0.5, 1.5, leaves).astype(np.float32) if weighted else None
+    hg = G.from_edges(leaves + 1, [(0, i) for i in range(1, leaves + 1)], w)
+    obj = pg.OBJ_WMOD if weighted else pg.OBJ_MOD
+    og, wg = _pair(mem, hg, obj)
+    vcmap = np.concatenate([[0, 0], np.arange(1, leaves, dtype=np.int32)]).astype(np.int32)
+    nc = leaves
+    co = O.build_coarse_graph(og, vcmap, nc)
+    cg = pg.build_coarse_graph(mem, wg, vcmap, nc)
+    for a, b in zip(co.arrays(), cg.to_host()):
+        assert np.array_equal(a, b)
+    rg = cg.to_host()[0]
+    assert rg[1] - rg[0] == leaves - 1
