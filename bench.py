@@ -41,7 +41,10 @@ METRIC = "Leiden edges/s at equal modularity: batched+learned vs plain, same B20
 UNIT = "edges/s"
 WORKLOAD = ("pLeiden+ until stable (ex_iters=-1), WMod, DC-SBM n=4,194,304, deg exp 2.5 min 5 mean 20, "
             "communities exp 1.5 on [50,5000], mu=0.4, FP32 weights U[0.5,1.5), int64 offsets")
-DOMINANT_FAMILIES = ("select_warp", "select_block", "afterburner_warp", "own_weights", "contract", "leiden_refine")
+DOMINANT_FAMILIES = ("select_warp", "select_block", "select_huge", "afterburner_warp", "own_weights", "contract",
+                     "leiden_refine", "filter")
+# sub-phases reported beside the families (not candidates for the roofline line)
+SUB_PHASES = ("contract_prep", "contract_hash", "contract_place", "contract_place_big", "host_alloc")
 
 
 def parse():
@@ -242,7 +245,7 @@ def ours(args):
     step(args.seed + rank)
     _lib.check(lib.pggc_profile_enable(mem.handle, 0))
     fam = {}
-    for f in DOMINANT_FAMILIES:
+    for f in DOMINANT_FAMILIES + SUB_PHASES:
         n_l, t_ms, by = (_lib.ctypes.c_int64(), _lib.ctypes.c_double(), _lib.ctypes.c_double())
         _lib.check(lib.pggc_profile_read(mem.handle, f.encode(), _lib.ctypes.byref(n_l), _lib.ctypes.byref(t_ms),
                                          _lib.ctypes.byref(by)))
@@ -280,7 +283,7 @@ def ours(args):
     e2e_value = world * m / (ms_e2e / 1000.0)
 
     # roofline for the dominant instrumented kernel
-    dom = max((f for f in fam if fam[f][2] > 0), key=lambda f: fam[f][1], default=None)
+    dom = max((f for f in DOMINANT_FAMILIES if fam[f][2] > 0), key=lambda f: fam[f][1], default=None)
     peak, peak_kind = peaks()
     roof = None
     if dom is not None:
@@ -314,7 +317,7 @@ def ours(args):
                    "modularity": q, "levels": stats["levels"], "passes": stats["passes"],
                    "sweeps": stats["sweeps"], "labels": stats["label_count"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "ms_per_step": ms_e2e},
+                "ms_per_step": ms_e2e, "ms_each": e2e_ms},
         "roofline": roof,
         "kernel_families": {f: {"launches": v[0], "ms": v[1], "alg_bytes": v[2]} for f, v in fam.items()},
         "cpu_baseline": cpu,

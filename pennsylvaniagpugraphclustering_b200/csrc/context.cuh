@@ -3,6 +3,7 @@
 // allocations from the device memory pool, pinned host scalars for the few
 // values the host must read, and a device error flag latched by bounded loops.
 #pragma once
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -82,6 +83,12 @@ struct Context {
         max_smem_optin = prop.sharedMemPerBlockOptin;
         PGGC_CUDA(cudaStreamSynchronize(stream));
     }
+    // Stack arena for short-lived temporaries (scan tile sums, reduction
+    // partials, sort histograms): LIFO reuse of one device buffer.  Work on the
+    // context is ordered on one stream, so a region may be handed out again
+    // as soon as the host has queued the kernels of its previous owner.
+    unsigned char* arena = nullptr;
+    size_t arena_cap = 0, arena_top = 0;
     // grow-only scratch slots reused across calls (one user at a time per slot)
     std::vector<std::pair<void*, size_t>> ws;
     template <class T>
@@ -102,6 +109,7 @@ struct Context {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& e : ws)
             if (e.first) cudaFreeAsync(e.first, stream);
+        if (arena) cudaFreeAsync(arena, stream);
         for (auto& pe : prof_pending) {
             cudaEventDestroy(pe.second.first);
             cudaEventDestroy(pe.second.second);
@@ -123,7 +131,17 @@ struct Context {
     T* alloc(i64 count) {
         if (count <= 0) count = 1;
         T* p = nullptr;
-        PGGC_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (size_t)count, stream));
+        if (profiling) {
+            // host time spent in the stream-ordered allocator (pool growth shows here)
+            auto t0 = std::chrono::steady_clock::now();
+            PGGC_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (size_t)count, stream));
+            auto& st = prof["host_alloc"];
+            st.launches++;
+            st.bytes += (double)(sizeof(T) * (size_t)count);
+            st.ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        } else {
+            PGGC_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (size_t)count, stream));
+        }
         return p;
     }
     void release(void* p) {
@@ -245,6 +263,40 @@ struct ProfScope {
         }
         nvtxRangePop();
     }
+};
+
+// A temporary of `count` T from the context's arena (released in LIFO order
+// when this object goes out of scope), or from the stream-ordered pool when
+// the arena has no room.  The arena is (re)sized to 64 MiB or the request,
+// whichever is larger, when it is empty.
+template <class T>
+struct Tmp {
+    Context& ctx;
+    T* p = nullptr;
+    size_t mark = 0;
+    bool pooled = false;
+    Tmp(Context& c, i64 count) : ctx(c) {
+        const size_t bytes = ((sizeof(T) * (size_t)(count > 0 ? count : 1)) + 255) & ~(size_t)255;
+        if (ctx.arena_top == 0 && ctx.arena_cap < bytes) {
+            if (ctx.arena) PGGC_CUDA(cudaFreeAsync(ctx.arena, ctx.stream));
+            ctx.arena_cap = std::max<size_t>(bytes, (size_t)64 << 20);
+            PGGC_CUDA(cudaMallocAsync((void**)&ctx.arena, ctx.arena_cap, ctx.stream));
+        }
+        if (ctx.arena_top + bytes <= ctx.arena_cap) {
+            mark = ctx.arena_top;
+            p = (T*)(ctx.arena + ctx.arena_top);
+            ctx.arena_top += bytes;
+        } else {
+            pooled = true;
+            p = ctx.alloc<T>(count);
+        }
+    }
+    ~Tmp() {
+        if (pooled) cudaFreeAsync(p, ctx.stream);
+        else ctx.arena_top = mark;
+    }
+    Tmp(const Tmp&) = delete;
+    Tmp& operator=(const Tmp&) = delete;
 };
 
 // RAII device buffer allocated on the context stream.

@@ -17,9 +17,10 @@
 //     with a global table for the rows that overflow it; weights are summed
 //     exactly (int64 / FP64);
 //  5. a prefix sum of the unique counts gives the coarse row offsets;
-//  6. each row is sorted by column (warp rank sort, block bitonic sort in shared
+//  6. each row is sorted by column (warp rank sort, block rank sort in shared
 //     memory, LSD radix sort for rows above 4096 entries) and written out.
 // The output is the canonical (row, col)-sorted coarse CSR.
+#include <optional>
 #include "kernels.cuh"
 
 namespace pggc {
@@ -408,49 +409,48 @@ __global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* li
     }
 }
 
+constexpr int PB_MID = 1024;
 constexpr int PB_MAX = 4096;
 
-template <class W>
-__global__ void __launch_bounds__(256) k_place_block(const i32* list, const i64* d_count, const i64* P, const i64* cstart,
-                                                     const i64* ucount, const i64* rowptr, const i32* skey,
-                                                     const typename Traits<W>::V* sval, i32* col, W* wout) {
-    using V = typename Traits<W>::V;
-    __shared__ i32 kk[PB_MAX];
-    __shared__ V vv[PB_MAX];
+// block per row of up to CAP entries: the keys are staged in shared memory and
+// every thread ranks its CAP / THREADS keys against all of them (the keys of a
+// row are distinct), then writes each entry at its rank.  u passes over
+// shared memory (broadcast reads) replace a bitonic network's log^2 barriers.
+template <class W, int THREADS, int CAP>
+__global__ void __launch_bounds__(THREADS) k_place_block(const i32* list, const i64* d_count, const i64* P,
+                                                         const i64* cstart, const i64* ucount, const i64* rowptr,
+                                                         const i32* skey, const typename Traits<W>::V* sval, i32* col,
+                                                         W* wout) {
+    constexpr int PER = CAP / THREADS;
+    __shared__ i32 kk[CAP];
     const i64 count = *d_count;
     for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
-        i32 c = list[x];
-        i64 src = P[cstart[c]];
-        i64 u = ucount[c];
-        u32 T = next_pow2_u32((u32)u);
-        for (u32 s = threadIdx.x; s < T; s += 256) {
-            kk[s] = s < u ? skey[src + s] : 2147483647;
-            vv[s] = s < u ? sval[src + s] : V(0);
-        }
+        const i32 c = list[x];
+        const i64 src = P[cstart[c]];
+        const int u = (int)ucount[c];
+        const i64 dst = rowptr[c];
+        for (int s = threadIdx.x; s < u; s += THREADS) kk[s] = skey[src + s];
         __syncthreads();
-        // bitonic sort of T keys (ascending)
-        for (u32 k = 2; k <= T; k <<= 1) {
-            for (u32 j = k >> 1; j > 0; j >>= 1) {
-                for (u32 t = threadIdx.x; t < T; t += 256) {
-                    u32 p = t ^ j;
-                    if (p > t) {
-                        bool up = (t & k) == 0;
-                        i32 a0 = kk[t], a1 = kk[p];
-                        if ((a0 > a1) == up) {
-                            kk[t] = a1;
-                            kk[p] = a0;
-                            V v0 = vv[t];
-                            vv[t] = vv[p];
-                            vv[p] = v0;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
+        i32 mk[PER];
+        int rk[PER];
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int s = threadIdx.x + q * THREADS;
+            mk[q] = s < u ? kk[s] : 2147483647;
+            rk[q] = 0;
         }
-        for (u32 s = threadIdx.x; s < u; s += 256) {
-            col[rowptr[c] + s] = kk[s];
-            wout[rowptr[c] + s] = to_w<W>(vv[s]);
+        for (int t = 0; t < u; t++) {
+            const i32 o = kk[t];
+#pragma unroll
+            for (int q = 0; q < PER; q++) rk[q] += o < mk[q] ? 1 : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int s = threadIdx.x + q * THREADS;
+            if (s < u) {
+                col[dst + rk[q]] = mk[q];
+                wout[dst + rk[q]] = to_w<W>(sval[src + s]);
+            }
         }
         __syncthreads();
     }
@@ -459,26 +459,27 @@ __global__ void __launch_bounds__(256) k_place_block(const i32* list, const i64*
 // big rows: gather into (row-major) temp with composite keys, radix sort, place
 template <class V>
 __global__ void k_big_gather(const i32* list, i64 count, const i64* tstart, const i64* P, const i64* cstart,
-                             const i64* ucount, const i32* skey, const V* sval, u64* tkey, V* tval) {
+                             const i64* ucount, const i32* skey, const V* sval, u64* tkey, V* tval, int cbits) {
     for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
         i32 c = list[x];
         i64 src = P[cstart[c]];
         i64 u = ucount[c];
         i64 dst = tstart[x];
         for (i64 s = threadIdx.x; s < u; s += blockDim.x) {
-            tkey[dst + s] = ((u64)x << 32) | (u64)(u32)skey[src + s];
+            tkey[dst + s] = ((u64)x << cbits) | (u64)(u32)skey[src + s];
             tval[dst + s] = sval[src + s];
         }
     }
 }
 template <class W>
 __global__ void k_big_place(const i32* list, i64 count, const i64* tstart, const i64* rowptr, const u64* tkey,
-                            const typename Traits<W>::V* tval, i32* col, W* wout) {
+                            const typename Traits<W>::V* tval, i32* col, W* wout, int cbits) {
+    const u64 cmask = ((u64)1 << cbits) - 1;
     for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
         i32 c = list[x];
         i64 a = tstart[x], b = tstart[x + 1];
         for (i64 y = a + threadIdx.x; y < b; y += blockDim.x) {
-            col[rowptr[c] + (y - a)] = (i32)(u32)(tkey[y] & 0xffffffffull);
+            col[rowptr[c] + (y - a)] = (i32)(u32)(tkey[y] & cmask);
             wout[rowptr[c] + (y - a)] = to_w<W>(tval[y]);
         }
     }
@@ -522,8 +523,8 @@ __global__ void k_bucket_rows(const i64* P, const i64* cstart, i64 nc, i32* l0, 
 }
 
 // Placement buckets by unique count u: 0: u <= 32, 1: u <= PW_MAX,
-// 2: u <= PB_MAX, 3: above (rows with no entries are skipped).
-__global__ void k_bucket_place(const i64* ucount, i64 nc, i32* l0, i32* l1, i32* l2, i32* l3,
+// 2: u <= PB_MID, 3: u <= PB_MAX, 4: above (rows with no entries are skipped).
+__global__ void k_bucket_place(const i64* ucount, i64 nc, i32* l0, i32* l1, i32* l2, i32* l3, i32* l4,
                                unsigned long long* cnt) {
     const int l = lane_id();
     for (i64 c0 = (blockIdx.x * (i64)blockDim.x + threadIdx.x) - l; c0 < nc; c0 += (i64)gridDim.x * blockDim.x) {
@@ -531,11 +532,11 @@ __global__ void k_bucket_place(const i64* ucount, i64 nc, i32* l0, i32* l1, i32*
         int k = -1;
         if (c < nc) {
             const i64 u = ucount[c];
-            k = u <= 0 ? -1 : u <= 32 ? 0 : u <= PW_MAX ? 1 : u <= PB_MAX ? 2 : 3;
+            k = u <= 0 ? -1 : u <= 32 ? 0 : u <= PW_MAX ? 1 : u <= PB_MID ? 2 : u <= PB_MAX ? 3 : 4;
         }
-        i32* lists[4] = {l0, l1, l2, l3};
+        i32* lists[5] = {l0, l1, l2, l3, l4};
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
+        for (int b = 0; b < 5; b++) {
             const unsigned m = __ballot_sync(FULL, k == b);
             if (!m) continue;
             const int leader = __ffs(m) - 1;
@@ -570,10 +571,26 @@ struct ListUIn {
     __device__ i64 operator()(i64 x) const { return x < *d_count ? u[list[x]] : 0; }
 };
 
+// Contraction temporaries live in grow-only workspace slots of the context
+// (sized by the largest level, reused by every later contraction), so the
+// level loop does not go through the allocator for them.
+enum ContractSlot : int {
+    CS_CNT = 50, CS_BOUND, CS_CSTART, CS_P, CS_UCOUNT, CS_MEMBERS, CS_MEMBERPOS, CS_CURSOR, CS_TOT, CS_FKEY, CS_FW,
+    CS_OKEY, CS_OVAL, CS_LW, CS_LM, CS_LB, CS_LB2, CS_LH, CS_LO, CS_COUNTS, CS_PW, CS_PR, CS_PB, CS_PB2, CS_PH,
+    CS_TSTART, CS_TK, CS_TK2, CS_TV, CS_TV2
+};
+template <class T>
+struct WsBuf {
+    T* p;
+    WsBuf(Context& c, int slot, i64 count) : p(c.ws_get<T>(slot, std::max<i64>(count, 1))) {}
+};
+
 template <class W>
 std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, const i32* vcmap, i64 nc) {
     using V = typename Traits<W>::V;
     ProfScope ps(ctx, "contract");
+    std::optional<ProfScope> phase;  // sub-phases: prep (count .. flatten), hash, place
+    phase.emplace(ctx, "contract_prep");
     auto cg = std::make_unique<Graph<W>>();
     cg->n = nc;
     cg->uniform = false;
@@ -587,9 +604,10 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         cg->w = DBuf<W>(ctx, 1);
         return cg;
     }
-    DBuf<i64> cnt(ctx, nc + 1), bound(ctx, nc + 1), cstart(ctx, nc + 1), P(ctx, n + 1), ucount(ctx, nc + 1);
-    DBuf<i32> members(ctx, n);
-    DBuf<i64> memberpos(ctx, n);
+    WsBuf<i64> cnt(ctx, CS_CNT, nc + 1), bound(ctx, CS_BOUND, nc + 1), cstart(ctx, CS_CSTART, nc + 1),
+        P(ctx, CS_P, n + 1), ucount(ctx, CS_UCOUNT, nc + 1);
+    WsBuf<i32> members(ctx, CS_MEMBERS, n);
+    WsBuf<i64> memberpos(ctx, CS_MEMBERPOS, n);
     PGGC_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(i64) * (nc + 1), ctx.stream));
     PGGC_CUDA(cudaMemsetAsync(bound.p, 0, sizeof(i64) * (nc + 1), ctx.stream));
     int gridv = (int)std::min<i64>(ceil_div(n, 256), (i64)ctx.num_sms * 16);
@@ -597,37 +615,37 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     PGGC_LAUNCH_CHECK();
     scan_apply(ctx, ArrIn{cnt.p}, ArrOutExcl{cstart.p}, nc + 1, nullptr, nullptr);
     {
-        DBuf<i64> cursor(ctx, nc + 1);
+        WsBuf<i64> cursor(ctx, CS_CURSOR, nc + 1);
         copy_d2d(ctx, cursor.p, cstart.p, nc + 1);
         k_scatter_members<<<gridv, 256, 0, ctx.stream>>>(vcmap, n, cursor.p, members.p, memberpos.p);
         PGGC_LAUNCH_CHECK();
     }
-    DBuf<i64> tot(ctx, 4);
+    WsBuf<i64> tot(ctx, CS_TOT, 4);
     scan_apply(ctx, MemberDegIn{gv.rowptr, members.p, n}, ArrOutExcl{P.p}, n + 1, nullptr, tot.p);
     // flattened rows: coarse key and weight of every fine edge at its flat position
-    DBuf<i32> fkey(ctx, std::max<i64>(g.nnz, 1));
-    DBuf<W> fw;
-    if (gv.w) fw = DBuf<W>(ctx, std::max<i64>(g.nnz, 1));
+    WsBuf<i32> fkey(ctx, CS_FKEY, g.nnz);
+    W* fw_p = gv.w ? ctx.ws_get<W>(CS_FW, std::max<i64>(g.nnz, 1)) : nullptr;
     if (g.nnz > 0) {
         int grid = (int)std::min<i64>(ceil_div(ceil_div(n, 32), 8), (i64)ctx.num_sms * 16);
-        k_flatten<W><<<grid, 256, 0, ctx.stream>>>(gv, vcmap, P.p, memberpos.p, fkey.p, fw.p);
+        k_flatten<W><<<grid, 256, 0, ctx.stream>>>(gv, vcmap, P.p, memberpos.p, fkey.p, fw_p);
         PGGC_LAUNCH_CHECK();
     }
     const i64 total_bound = g.nnz;
-    DBuf<i32> okey(ctx, std::max<i64>(total_bound, 1));
-    DBuf<V> oval(ctx, std::max<i64>(total_bound, 1));
+    WsBuf<i32> okey(ctx, CS_OKEY, total_bound);
+    WsBuf<V> oval(ctx, CS_OVAL, total_bound);
 
     // bucket lists by bound (sum of member degrees) and table size U =
     // min(bound, nc): small warp rows (bound <= 32), medium warp rows
     // (bound <= 256), block rows with shared tables of 2048 slots (U <= 1024)
     // and 8192 slots (U <= 4096), big rows with 16384-slot shared tables
     // (U > 4096) whose overflow falls back to global tables
-    DBuf<i32> lw(ctx, nc), lm(ctx, nc), lb(ctx, nc), lb2(ctx, nc), lh(ctx, nc), lo(ctx, nc);
+    WsBuf<i32> lw(ctx, CS_LW, nc), lm(ctx, CS_LM, nc), lb(ctx, CS_LB, nc), lb2(ctx, CS_LB2, nc), lh(ctx, CS_LH, nc),
+        lo(ctx, CS_LO, nc);
     // counts: [0] small warp rows, [1] medium warp rows, [2] 2048-slot block
     // rows, [3] 8192-slot block rows, [4] big rows, [5] largest big-row bound,
-    // [6] overflow rows, [7..10] placement buckets, [11] coarse nnz,
-    // [12] big-row placement total
-    DBuf<i64> counts(ctx, 16);
+    // [6] overflow rows, [7..11] placement buckets, [12] big-row placement
+    // total, [14] coarse nnz
+    WsBuf<i64> counts(ctx, CS_COUNTS, 16);
     PGGC_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(i64) * 16, ctx.stream));
     {
         int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(nc, 256), (i64)ctx.num_sms * 8));
@@ -646,7 +664,7 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     a.members = members.p;
     a.P = P.p;
     a.fkey = fkey.p;
-    a.fw = fw.p;
+    a.fw = fw_p;
     a.out_key = okey.p;
     a.out_val = oval.p;
     a.ucount = ucount.p;
@@ -664,6 +682,8 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         k_contract_warp<W, 512, WARPS><<<grid, WARPS * 32, 0, ctx.stream>>>(a, lm.p, counts.p + 1);
         PGGC_LAUNCH_CHECK();
     }
+    phase.reset();
+    phase.emplace(ctx, "contract_hash");
     const size_t slot = sizeof(V) + sizeof(i32);
     if (n_b > 0) {
         constexpr int TS = 2048;
@@ -689,31 +709,36 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         k_contract_block<W, false, 1024, true><<<grid, 1024, slot * TS, ctx.stream>>>(
             a, lh.p, counts.p + 4, nullptr, nullptr, TS, nc, lo.p, counts.p + 6);
         PGGC_LAUNCH_CHECK();
-        // global tables sized for the largest table among the big rows, one
-        // region per resident block, at most 2 GiB of tables; the blocks
-        // beyond the overflow count exit at once
-        i64 maxb = std::min<i64>(max_huge, nc);
-        i64 gcap = next_pow2_u32((u32)std::min<i64>(2 * std::max<i64>(maxb, 1), (i64)1 << 30));
-        i64 by_mem = std::max<i64>(1, ((i64)2 << 30) / (gcap * (i64)slot));
-        int ggrid = (int)std::min<i64>(std::min<i64>(n_h, (i64)ctx.num_sms * 2), by_mem);
-        i32* gk = ctx.ws_get<i32>(WS_CONTRACT_GK, gcap * ggrid);
-        V* gvv = ctx.ws_get<V>(WS_CONTRACT_GV, gcap * ggrid);
-        k_contract_block<W, true><<<ggrid, 256, 0, ctx.stream>>>(a, lo.p, counts.p + 6, gk, gvv, gcap, nc);
-        PGGC_LAUNCH_CHECK();
+        // rows that overflowed: global tables sized for the largest table
+        // among the big rows, one region per resident block, at most 2 GiB of
+        // tables (allocated only when some row overflowed)
+        const i64 n_ovf = ctx.read1(counts.p + 6);
+        if (n_ovf > 0) {
+            i64 maxb = std::min<i64>(max_huge, nc);
+            i64 gcap = next_pow2_u32((u32)std::min<i64>(2 * std::max<i64>(maxb, 1), (i64)1 << 30));
+            i64 by_mem = std::max<i64>(1, ((i64)2 << 30) / (gcap * (i64)slot));
+            int ggrid = (int)std::min<i64>(std::min<i64>(n_ovf, (i64)ctx.num_sms * 2), by_mem);
+            i32* gk = ctx.ws_get<i32>(WS_CONTRACT_GK, gcap * ggrid);
+            V* gvv = ctx.ws_get<V>(WS_CONTRACT_GV, gcap * ggrid);
+            k_contract_block<W, true><<<ggrid, 256, 0, ctx.stream>>>(a, lo.p, counts.p + 6, gk, gvv, gcap, nc);
+            PGGC_LAUNCH_CHECK();
+        }
     }
     // coarse row offsets, placement buckets and the big-row total, then one round trip
-    scan_apply(ctx, UcountIn{ucount.p, nc}, RowptrOut{cg->rowptr.p}, nc + 1, nullptr, counts.p + 11);
-    DBuf<i32> pw(ctx, nc), pr(ctx, nc), pb(ctx, nc), ph(ctx, nc);
+    phase.reset();
+    phase.emplace(ctx, "contract_place");
+    scan_apply(ctx, UcountIn{ucount.p, nc}, RowptrOut{cg->rowptr.p}, nc + 1, nullptr, counts.p + 14);
+    WsBuf<i32> pw(ctx, CS_PW, nc), pr(ctx, CS_PR, nc), pb(ctx, CS_PB, nc), pb2(ctx, CS_PB2, nc), ph(ctx, CS_PH, nc);
     {
         int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(nc, 256), (i64)ctx.num_sms * 8));
-        k_bucket_place<<<grid, 256, 0, ctx.stream>>>(ucount.p, nc, pw.p, pr.p, pb.p, ph.p,
+        k_bucket_place<<<grid, 256, 0, ctx.stream>>>(ucount.p, nc, pw.p, pr.p, pb.p, pb2.p, ph.p,
                                                     (unsigned long long*)(counts.p + 7));
         PGGC_LAUNCH_CHECK();
     }
-    DBuf<i64> tstart(ctx, nc + 1);
-    scan_apply(ctx, ListUIn{ph.p, ucount.p, counts.p + 10}, ArrOutExcl{tstart.p}, nc + 1, nullptr, counts.p + 12);
+    WsBuf<i64> tstart(ctx, CS_TSTART, nc + 1);
+    scan_apply(ctx, ListUIn{ph.p, ucount.p, counts.p + 11}, ArrOutExcl{tstart.p}, nc + 1, nullptr, counts.p + 12);
     const i64* pc = (const i64*)ctx.readback(counts.p, 16 * sizeof(i64));
-    const i64 p_w = pc[7], p_r = pc[8], p_b = pc[9], p_h = pc[10], nnz_c = pc[11], tn = pc[12];
+    const i64 p_w = pc[7], p_r = pc[8], p_b = pc[9], p_b2 = pc[10], p_h = pc[11], nnz_c = pc[14], tn = pc[12];
     ctx.check_device_error();
     cg->nnz = nnz_c;
     cg->col = DBuf<i32>(ctx, std::max<i64>(nnz_c, 1));
@@ -732,24 +757,36 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         PGGC_LAUNCH_CHECK();
     }
     if (p_b > 0) {
-        int grid = (int)std::min<i64>(p_b, (i64)ctx.num_sms * 4);
-        k_place_block<W><<<grid, 256, 0, ctx.stream>>>(pb.p, counts.p + 9, P.p, cstart.p, ucount.p, cg->rowptr.p,
-                                                       okey.p, oval.p, cg->col.p, cg->w.p);
+        int grid = (int)std::min<i64>(p_b, (i64)ctx.num_sms * 8);
+        k_place_block<W, 256, PB_MID><<<grid, 256, 0, ctx.stream>>>(pb.p, counts.p + 9, P.p, cstart.p, ucount.p,
+                                                                    cg->rowptr.p, okey.p, oval.p, cg->col.p, cg->w.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    if (p_b2 > 0) {
+        int grid = (int)std::min<i64>(p_b2, (i64)ctx.num_sms * 2);
+        k_place_block<W, 1024, PB_MAX><<<grid, 1024, 0, ctx.stream>>>(pb2.p, counts.p + 10, P.p, cstart.p, ucount.p,
+                                                                      cg->rowptr.p, okey.p, oval.p, cg->col.p,
+                                                                      cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
     if (p_h > 0) {
-        DBuf<u64> tk(ctx, tn), tk2(ctx, tn);
-        DBuf<V> tv(ctx, tn), tv2(ctx, tn);
+        WsBuf<u64> tk(ctx, CS_TK, tn), tk2(ctx, CS_TK2, tn);
+        WsBuf<V> tv(ctx, CS_TV, tn), tv2(ctx, CS_TV2, tn);
         int grid = (int)std::min<i64>(p_h, (i64)ctx.num_sms * 4);
+        ProfScope pbig(ctx, "contract_place_big");
+        ctx.prof_add_bytes("contract_place_big", (double)tn);
+        // composite key (row rank, column): column bits for ids < nc only
+        const int cbits = std::max(1, bits_for((u64)(nc - 1)));
         k_big_gather<V><<<grid, 256, 0, ctx.stream>>>(ph.p, p_h, tstart.p, P.p, cstart.p, ucount.p, okey.p, oval.p,
-                                                      tk.p, tv.p);
+                                                      tk.p, tv.p, cbits);
         PGGC_LAUNCH_CHECK();
-        int hib = 32 + bits_for((u64)p_h);
+        int hib = cbits + bits_for((u64)p_h);
         radix_sort_pairs<V>(ctx, tk.p, tv.p, tn, 0, hib, tk2.p, tv2.p);
         k_big_place<W><<<grid, 256, 0, ctx.stream>>>(ph.p, p_h, tstart.p, cg->rowptr.p, tk.p, tv.p, cg->col.p,
-                                                     cg->w.p);
+                                                     cg->w.p, cbits);
         PGGC_LAUNCH_CHECK();
     }
+    phase.reset();
     // algorithmic bytes: per fine edge its column, weight, the map of its head
     // and one table insert (key + value); per fine vertex its offset and map;
     // the coarse CSR written once

@@ -174,6 +174,50 @@ __global__ void __launch_bounds__(256) k_pick_heavy_warp(PickArgs<W> a, const i3
     }
 }
 
+// G-lane groups for low-degree vertices (NG = 32 / G vertices per warp); the
+// argmax order (sample, then edge index) is total, so any split of the edges
+// over lanes gives the warp kernel's pick
+template <class W, int G>
+__global__ void __launch_bounds__(256) k_pick_heavy_grp(PickArgs<W> a, const i32* list, i64 count) {
+    constexpr int NG = 32 / G;
+    const int l = lane_id(), r = l & (G - 1), grp = l / G;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 base = gw * NG; base < count; base += nw * NG) {
+        const i64 x = base + grp;
+        i32 i = -1;
+        bool act = false;
+        i64 b = 0, e = 0;
+        float multi = 0.f;
+        if (x < count) {
+            i = list[x];
+            const u32 h = murmur3_32(a.seed + (u32)i);
+            if (h % 10000u == 0 || !a.well[i]) {
+                if (r == 0) a.hn[i] = i;
+            } else {
+                act = true;
+                b = a.g.rowptr[i];
+                e = a.g.rowptr[i + 1];
+                multi = a.gamma * to_f(a.g.vtx_w[i]);
+            }
+        }
+        float bs = -1.0f;
+        i64 bj = -1;
+        if (act)
+            for (i64 j = b + r; j < e; j += G) heavy_eval(a, i, j, multi, bs, bj);
+#pragma unroll
+        for (int d = G / 2; d >= 1; d >>= 1) {
+            float os = __shfl_xor_sync(FULL, bs, d);
+            i64 oj = __shfl_xor_sync(FULL, bj, d);
+            if (sample_better(os, oj, bs, bj)) {
+                bs = os;
+                bj = oj;
+            }
+        }
+        if (r == 0 && act) a.hn[i] = bj >= b ? a.g.col[bj] : i;
+    }
+}
+
 template <class W>
 __global__ void __launch_bounds__(1024) k_pick_heavy_block(PickArgs<W> a, const i32* list, i64 count) {
     __shared__ float ws[32];
@@ -487,8 +531,14 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
             PGGC_LAUNCH_CHECK();
         }
     } else {
-        if (nsmall > 0) {
-            k_pick_heavy_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list, nsmall);
+        // degree < 128: 8-lane groups; 128 <= degree < 15000: a warp per vertex
+        if (ord.off_large > 0) {
+            const int g8 = (int)std::min<i64>(ceil_div(ord.off_large, 32), (i64)ctx.num_sms * 16);
+            k_pick_heavy_grp<W, 8><<<g8, 256, 0, ctx.stream>>>(pa, small_list, ord.off_large);
+            PGGC_LAUNCH_CHECK();
+        }
+        if (nsmall > ord.off_large) {
+            k_pick_heavy_warp<W><<<gw, 256, 0, ctx.stream>>>(pa, small_list + ord.off_large, nsmall - ord.off_large);
             PGGC_LAUNCH_CHECK();
         }
         if (nmass > 0) {

@@ -219,6 +219,47 @@ __device__ __forceinline__ void chunk_to_table(const SelArgs<W>& a, const VCtx& 
     if (leader) table_add(keys, vals, mask, c, s, a.err, a.probe_cap);
 }
 
+// Insert that gives up after TRY_PROBES probes (the caller sends the vertex
+// to the global-table pass); a run that long means the table is nearly full.
+constexpr u32 TRY_PROBES = 64;
+template <class V>
+__device__ __forceinline__ bool table_try_add(i32* keys, V* vals, u32 mask, i32 c, V x) {
+    u32 s = xorshift32((u32)c) & mask;
+    volatile i32* vk = keys;
+    for (u32 probe = 0; probe < TRY_PROBES && probe <= mask; probe++) {
+        i32 k = vk[s];
+        if (k == c) {
+            vatomic_add(&vals[s], x);
+            return true;
+        }
+        if (k == -1) {
+            i32 old = atomicCAS(&keys[s], -1, c);
+            if (old == -1 || old == c) {
+                vatomic_add(&vals[s], x);
+                return true;
+            }
+        }
+        s = (s + 1) & mask;
+    }
+    return false;
+}
+
+// chunk_to_table with table_try_add: false if this lane's insert failed
+template <class W>
+__device__ __forceinline__ bool chunk_to_table_try(const SelArgs<W>& a, const VCtx& vc, i64 j, i64 e, i32* keys,
+                                                   typename Traits<W>::V* vals, u32 mask) {
+    using V = typename Traits<W>::V;
+    bool valid = j < e;
+    i32 c = valid ? a.part[a.g.col[j]] : -1;
+    V wv = valid ? V(a.g.wgt(j)) : V(0);
+    bool keep = valid && c != vc.p;
+    i32 key = keep ? c : (i32)(0x80000000u | lane_id());
+    unsigned peers = __match_any_sync(FULL, key);
+    bool leader = keep && ((peers & lanemask_lt()) == 0);
+    V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
+    return leader ? table_try_add(keys, vals, mask, c, s) : true;
+}
+
 // ---- warp per vertex, degree < 128 (order1 bucket 0) ----------------------
 constexpr int SELW_WARPS = 8;
 constexpr int SELW_T = 256;
@@ -378,8 +419,10 @@ __device__ __forceinline__ void group_best(Best& b) {
 }
 
 // G-lane groups, one vertex each, for vertices of degree <= G (single chunk):
-// class k of the class lists.
-template <class W, bool CON, int G>
+// class k of the class lists.  Each group takes UV vertices per iteration and
+// issues their loads together (the chains list -> row -> column -> label ->
+// volume are latency-bound, so independent vertices in flight set the pace).
+template <class W, bool CON, int G, int UV = 2>
 __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls, const i64* off, int k) {
     using V = typename Traits<W>::V;
     constexpr int NG = 32 / G;
@@ -388,39 +431,64 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
     unsigned long long pb = 0;
-    for (i64 base = lo + gw * NG; base < hi; base += nw * NG) {
-        const i64 x = base + grp;
-        i32 i = -1;
-        bool act = false;
-        if (x < hi) {
-            i = cls[x];
-            act = a.dest[i] != NO_MOVE;
+    for (i64 base = lo + gw * NG * UV; base < hi; base += nw * NG * UV) {
+        i32 iv[UV];
+        bool act[UV];
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            const i64 x = base + u * NG + grp;
+            iv[u] = x < hi ? cls[x] : -1;
         }
-        VCtx vc{};
-        i64 b = 0, e = 0;
-        if (act) {
-            vc = sel_prologue(a, i);
-            b = a.g.rowptr[i];
-            e = a.g.rowptr[i + 1];
+#pragma unroll
+        for (int u = 0; u < UV; u++) act[u] = iv[u] >= 0 && a.dest[iv[u]] != NO_MOVE;
+        VCtx vc[UV];
+        i64 b[UV], e[UV];
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            b[u] = 0;
+            e[u] = 0;
+            vc[u] = VCtx{};
+            if (act[u]) {
+                vc[u] = sel_prologue(a, iv[u]);
+                b[u] = a.g.rowptr[iv[u]];
+                e[u] = a.g.rowptr[iv[u] + 1];
+            }
+            if (r == 0 && iv[u] >= 0) pb += sel_bytes(a, e[u] - b[u], act[u]);
         }
-        if (r == 0 && x < hi) pb += sel_bytes(a, e - b, act);
-        Best best = none_best();
-        const i64 j = b + r;
-        const bool valid = act && j < e;
         if (a.initial) {
-            if (valid) sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
+#pragma unroll
+            for (int u = 0; u < UV; u++) {
+                Best best = none_best();
+                const i64 j = b[u] + r;
+                if (act[u] && j < e[u]) sel_eval<W, CON>(a, vc[u], a.g.col[j], V(a.g.wgt(j)), best);
+                group_best<G>(best);
+                if (r == 0 && act[u]) sel_finish(a, iv[u], vc[u], best);
+            }
         } else {
-            i32 c = valid ? a.part[a.g.col[j]] : -1;
-            V wv = valid ? V(a.g.wgt(j)) : V(0);
-            bool keep = valid && c != vc.p;
-            u64 key = keep ? (((u64)grp << 32) | (u64)(u32)c) : (0xFFFFFFFF00000000ull | (u64)l);
-            unsigned peers = __match_any_sync(FULL, key);
-            bool leader = keep && ((peers & lanemask_lt()) == 0);
-            V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
-            if (leader) sel_eval<W, CON>(a, vc, c, s, best);
+            i32 c[UV];
+            V wv[UV];
+#pragma unroll
+            for (int u = 0; u < UV; u++) {
+                const i64 j = b[u] + r;
+                const bool valid = act[u] && j < e[u];
+                c[u] = valid ? a.g.col[j] : -1;
+                wv[u] = valid ? V(a.g.wgt(j)) : V(0);
+            }
+#pragma unroll
+            for (int u = 0; u < UV; u++) c[u] = c[u] >= 0 ? a.part[c[u]] : -1;
+#pragma unroll
+            for (int u = 0; u < UV; u++) {
+                Best best = none_best();
+                const bool keep = c[u] >= 0 && c[u] != vc[u].p;
+                u64 key = keep ? (((u64)grp << 32) | (u64)(u32)c[u]) : (0xFFFFFFFF00000000ull | (u64)l);
+                unsigned peers = __match_any_sync(FULL, key);
+                bool leader = keep && ((peers & lanemask_lt()) == 0);
+                V sum = a.g.w ? group_sum<V>(peers, wv[u], leader) : V(__popc(peers));
+                if (leader) sel_eval<W, CON>(a, vc[u], c[u], sum, best);
+                group_best<G>(best);
+                if (r == 0 && act[u]) sel_finish(a, iv[u], vc[u], best);
+            }
         }
-        group_best<G>(best);
-        if (r == 0 && act) sel_finish(a, i, vc, best);
     }
     if (a.prof) {
         pb = (unsigned long long)warp_sum_i64((i64)pb);
@@ -429,13 +497,18 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
 }
 
 // ---- block per vertex, shared or global table -------------------------------
-template <class W, bool CON, bool GLOBAL, int THREADS = 256>
+// With OVF (vertices above HUGE_DEG, shared tables of gcap slots that may be
+// smaller than 2 * degree), a vertex whose distinct neighbour clusters do not
+// fit is appended to `ovf_list` for the global-table pass instead.
+template <class W, bool CON, bool GLOBAL, int THREADS = 256, bool OVF = false>
 __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg, i32* gkeys,
-                                                          typename Traits<W>::V* gvals, i64 gcap) {
+                                                          typename Traits<W>::V* gvals, i64 gcap,
+                                                          i32* ovf_list = nullptr, i64* ovf_count = nullptr) {
     using V = typename Traits<W>::V;
     constexpr int NW = THREADS / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Best wb[NW];
+    __shared__ int full;
     V* svals = (V*)smem_raw;
     i32* skeys = (i32*)(smem_raw + sizeof(V) * (GLOBAL ? 0 : gcap));  // gcap = shared table slots
     const int l = lane_id(), w = threadIdx.x >> 5;
@@ -446,12 +519,11 @@ __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg
     for (i64 x = lo + blockIdx.x; x < count; x += gridDim.x) {
         i32 i = rg.list[x];
         i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
-        if (!GLOBAL && e - b > HUGE_DEG) continue;
+        if (!GLOBAL && !OVF && e - b > HUGE_DEG) continue;
         if (a.dest[i] == NO_MOVE) {
             pb += sel_bytes(a, 0, false);
             continue;
         }
-        pb += sel_bytes(a, e - b, true);
         VCtx vc = sel_prologue(a, i);
         Best best = none_best();
         if (a.initial) {
@@ -460,18 +532,38 @@ __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg
         } else {
             i64 U = min(e - b, *a.label_count);
             u32 T = next_pow2_u32((u32)(2 * U));
+            if (OVF && T > (u32)gcap) T = (u32)gcap;
             for (u32 s = threadIdx.x; s < T; s += THREADS) {
                 keys[s] = -1;
                 vals[s] = V(0);
             }
+            if (OVF && threadIdx.x == 0) full = 0;
             __syncthreads();
-            for (i64 j = b + (i64)w * 32 + l; j - l < e; j += THREADS) chunk_to_table(a, vc, j, e, keys, vals, T - 1);
+            if (OVF) {
+                for (i64 j = b + (i64)w * 32 + l; j - l < e; j += THREADS) {
+                    if (!chunk_to_table_try(a, vc, j, e, keys, vals, T - 1)) full = 1;
+                    if (__any_sync(FULL, *(volatile int*)&full != 0)) break;
+                }
+                __syncthreads();
+                if (full) {
+                    if (threadIdx.x == 0) {
+                        i64 k = (i64)atomicAdd((unsigned long long*)ovf_count, 1ull);
+                        ovf_list[k] = i;
+                    }
+                    __syncthreads();
+                    continue;
+                }
+            } else {
+                for (i64 j = b + (i64)w * 32 + l; j - l < e; j += THREADS)
+                    chunk_to_table(a, vc, j, e, keys, vals, T - 1);
+            }
             __syncthreads();
             for (u32 s = threadIdx.x; s < T; s += THREADS) {
                 i32 c = keys[s];
                 if (c != -1) sel_eval<W, CON>(a, vc, c, vals[s], best);
             }
         }
+        pb += sel_bytes(a, e - b, true);
         warp_best(best);
         if (l == 0) wb[w] = best;
         __syncthreads();
@@ -585,6 +677,78 @@ __global__ void __launch_bounds__(256) k_own_grp(DGraph<W> g, const i32* lab, ty
     }
 }
 
+// Own-cluster weights of vertices of degree <= K * G: lane r of a G-lane group
+// adds the terms of edges r, r + G, ... (at most K) in that order, then the
+// group's xor butterfly -- the canonical association.  Each group takes UV
+// vertices per iteration and issues their loads together.
+template <class W, int G, int K, int UV = 2>
+__global__ void __launch_bounds__(256) k_own_small(DGraph<W> g, const i32* lab, typename Traits<W>::V* out, Range rg,
+                                                   int mode, unsigned char* flags, i32* dest,
+                                                   unsigned long long* prof) {
+    using V = typename Traits<W>::V;
+    constexpr int NG = 32 / G;
+    const int l = lane_id(), r = l & (G - 1), grp = l / G;
+    const i64 lo = rg.begin(), hi = rg.end();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    unsigned long long pb = 0;
+    for (i64 base = lo + gw * NG * UV; base < hi; base += nw * NG * UV) {
+        i32 iv[UV];
+        bool act[UV];
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            const i64 x = base + u * NG + grp;
+            iv[u] = x < hi ? rg.list[x] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < UV; u++) act[u] = iv[u] >= 0 && (mode == 0 || flags[iv[u]]);
+        i64 b[UV], e[UV];
+        i32 li[UV];
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            b[u] = act[u] ? g.rowptr[iv[u]] : 0;
+            e[u] = act[u] ? g.rowptr[iv[u] + 1] : 0;
+            li[u] = act[u] ? lab[iv[u]] : 0;
+        }
+        i32 cv[UV][K];
+        V wv[UV][K];
+#pragma unroll
+        for (int u = 0; u < UV; u++)
+#pragma unroll
+            for (int t = 0; t < K; t++) {
+                const i64 j = b[u] + r + (i64)t * G;
+                const bool valid = j < e[u];
+                cv[u][t] = valid ? g.col[j] : -1;
+                wv[u][t] = valid ? V(g.wgt(j)) : V(0);
+            }
+#pragma unroll
+        for (int u = 0; u < UV; u++)
+#pragma unroll
+            for (int t = 0; t < K; t++) cv[u][t] = cv[u][t] >= 0 ? lab[cv[u][t]] : -1;
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            V acc = V(0);
+#pragma unroll
+            for (int t = 0; t < K; t++)
+                if (b[u] + r + (i64)t * G < e[u]) acc += cv[u][t] == li[u] ? wv[u][t] : V(0);
+#pragma unroll
+            for (int d = G / 2; d >= 1; d >>= 1) acc = acc + __shfl_xor_sync(FULL, acc, d);
+            if (r == 0 && act[u]) {
+                out[iv[u]] = acc;
+                if (mode == 1) {
+                    dest[iv[u]] = NULL_PART;
+                    flags[iv[u]] = 0;
+                }
+                pb += 4 + 16 + 4 + sizeof(V) + (unsigned long long)(e[u] - b[u]) * (8 + (g.w ? sizeof(W) : 0));
+            }
+        }
+    }
+    if (prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (l == 0 && pb) atomicAdd(prof, pb);
+    }
+}
+
 template <class W>
 void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* lab,
                       typename Traits<W>::V* out, int mode, unsigned char* flags, i32* dest,
@@ -601,14 +765,17 @@ void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, cons
     const i64 c01 = cls->count;  // host upper bound of every class range
     if (c01 > 0) {
         int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(c01, 32), (i64)ctx.num_sms * 16));
-        k_own_grp<W, 8><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 0, cls->off + 2),
-                                                       mode, flags, dest, prof);
+        k_own_small<W, 8, 2><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
+                                                            dev_range(cls->list, cls->off + 0, cls->off + 2), mode,
+                                                            flags, dest, prof);
         PGGC_LAUNCH_CHECK();
-        k_own_grp<W, 16><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 2, cls->off + 3),
-                                                        mode, flags, dest, prof);
+        k_own_small<W, 16, 2><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
+                                                             dev_range(cls->list, cls->off + 2, cls->off + 3), mode,
+                                                             flags, dest, prof);
         PGGC_LAUNCH_CHECK();
-        k_own_grp<W, 32><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 3, cls->off + 4),
-                                                        mode, flags, dest, prof);
+        k_own_small<W, 32, 4><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
+                                                             dev_range(cls->list, cls->off + 3, cls->off + 4), mode,
+                                                             flags, dest, prof);
         PGGC_LAUNCH_CHECK();
     }
     if (ord.off_large2 > ord.off_large) {
@@ -711,6 +878,67 @@ __global__ void __launch_bounds__(256) k_afterburner_grp(ABArgs<W> a, Range rg) 
         if (r == 0 && act) {
             a.keep[i] = (igain + (float)ch) >= 0.0f ? 1 : 0;
             pb += ab_bytes(a, e - b);
+        }
+    }
+    if (a.prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (l == 0 && pb) atomicAdd(a.prof, pb);
+    }
+}
+
+// Afterburner for candidates of degree <= K * G, UV vertices per group per
+// iteration, canonical association as in k_own_small.
+template <class W, int G, int K, int UV = 2>
+__global__ void __launch_bounds__(256) k_afterburner_small(ABArgs<W> a, Range rg) {
+    constexpr int NG = 32 / G;
+    const int l = lane_id(), r = l & (G - 1), grp = l / G;
+    const i64 lo = rg.begin(), hi = rg.end();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    unsigned long long pb = 0;
+    for (i64 base = lo + gw * NG * UV; base < hi; base += nw * NG * UV) {
+        i32 iv[UV], bestv[UV], pv[UV], hv[UV];
+        bool act[UV];
+        float multi[UV], igain[UV];
+        i64 b[UV], e[UV];
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            const i64 x = base + u * NG + grp;
+            iv[u] = x < hi ? rg.list[x] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            bestv[u] = iv[u] >= 0 ? a.dest[iv[u]] : NO_MOVE;
+            act[u] = bestv[u] != NO_MOVE;
+        }
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            pv[u] = act[u] ? a.part[iv[u]] : 0;
+            multi[u] = act[u] ? to_f(a.g.vtx_w[iv[u]]) * a.pm : 0.f;
+            igain[u] = act[u] ? a.gain[iv[u]] : 0.f;
+            hv[u] = act[u] ? (i32)xorshift32((u32)iv[u]) : 0;
+            b[u] = act[u] ? a.g.rowptr[iv[u]] : 0;
+            e[u] = act[u] ? a.g.rowptr[iv[u] + 1] : 0;
+        }
+        double acc[UV];
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            acc[u] = 0.0;
+#pragma unroll
+            for (int t = 0; t < K; t++) {
+                const i64 j = b[u] + r + (i64)t * G;
+                if (j < e[u]) acc[u] += ab_term(a, j, pv[u], bestv[u], multi[u], igain[u], hv[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UV; u++) {
+            double ch = acc[u];
+#pragma unroll
+            for (int d = G / 2; d >= 1; d >>= 1) ch = ch + __shfl_xor_sync(FULL, ch, d);
+            if (r == 0 && act[u]) {
+                a.keep[iv[u]] = (igain[u] + (float)ch) >= 0.0f ? 1 : 0;
+                pb += ab_bytes(a, e[u] - b[u]);
+            }
         }
     }
     if (a.prof) {
@@ -1171,7 +1399,7 @@ struct Mover {
     View<i32> moved_at, csize;
 
     enum Slot { S_PART, S_DEST, S_CAND, S_MOVES, S_NEWL, S_AVAIL, S_PRIO, S_GAIN, S_PV, S_PVC, S_TD, S_FLAGS, S_KEEP,
-                S_HAS, S_SC, S_GK, S_GV, S_CLS, S_CLS_OFF, S_CLS_CNT, S_MOVED_AT, S_CSIZE };
+                S_HAS, S_SC, S_GK, S_GV, S_CLS, S_CLS_OFF, S_CLS_CNT, S_MOVED_AT, S_CSIZE, S_OVF, S_OVF_CNT };
 
     Mover(Context& c, const Graph<W>& gr, const Ordering& o, i64 capacity)
         : ctx(c), g(gr), ord(o), n(gr.n), cap(capacity) {
@@ -1323,9 +1551,21 @@ struct Mover {
         if (ord.n_huge > 0) {
             ProfScope ps(ctx, "select_huge");
             a.prof = ctx.prof_counter("select_huge");
-            int grid = (int)std::min<i64>(ord.n_huge, 32);
-            k_select_block<W, CON, true><<<grid, 256, 0, ctx.stream>>>(a, host_range(ord.huge.p, 0, ord.n_huge), gkeys.p,
-                                                                       gvals.p, gcap);
+            // 1024-thread blocks with 16384-slot shared tables; vertices with
+            // more distinct neighbour clusters than fit go to the global pass
+            const size_t slot = sizeof(V) + sizeof(i32);
+            constexpr int TS = 16384;
+            i32* ovf = ctx.ws_get<i32>(S_OVF, ord.n_huge);
+            i64* ovf_cnt = ctx.ws_get<i64>(S_OVF_CNT, 1);
+            PGGC_CUDA(cudaMemsetAsync(ovf_cnt, 0, sizeof(i64), ctx.stream));
+            set_dynamic_smem_once(k_select_block<W, CON, false, 1024, true>, (int)(slot * TS), ctx.device);
+            int grid = (int)std::min<i64>(ord.n_huge, (i64)ctx.num_sms);
+            k_select_block<W, CON, false, 1024, true><<<grid, 1024, slot * TS, ctx.stream>>>(
+                a, host_range(ord.huge.p, 0, ord.n_huge), nullptr, nullptr, TS, ovf, ovf_cnt);
+            PGGC_LAUNCH_CHECK();
+            int ggrid = (int)std::min<i64>(ord.n_huge, 32);
+            k_select_block<W, CON, true><<<ggrid, 256, 0, ctx.stream>>>(a, Range{ovf, nullptr, ovf_cnt, 0, 0}, gkeys.p,
+                                                                        gvals.p, gcap);
             PGGC_LAUNCH_CHECK();
         }
     }
@@ -1361,11 +1601,14 @@ struct Mover {
             ProfScope ps(ctx, "afterburner_warp");
             if (cls.count > 0) {
                 int grid = grid_for(ctx, ceil_div(cls.count, 32), 1, 16);
-                k_afterburner_grp<W, 8><<<grid, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 0, cls.off + 2));
+                k_afterburner_small<W, 8, 2><<<grid, 256, 0, ctx.stream>>>(
+                    a, dev_range(cls.list, cls.off + 0, cls.off + 2));
                 PGGC_LAUNCH_CHECK();
-                k_afterburner_grp<W, 16><<<grid, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 2, cls.off + 3));
+                k_afterburner_small<W, 16, 2><<<grid, 256, 0, ctx.stream>>>(
+                    a, dev_range(cls.list, cls.off + 2, cls.off + 3));
                 PGGC_LAUNCH_CHECK();
-                k_afterburner_grp<W, 32><<<grid, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 3, cls.off + 4));
+                k_afterburner_small<W, 32, 4><<<grid, 256, 0, ctx.stream>>>(
+                    a, dev_range(cls.list, cls.off + 3, cls.off + 4));
                 PGGC_LAUNCH_CHECK();
             }
             if (ord.off_large2 > ord.off_large) {

@@ -140,7 +140,7 @@ void scan_apply(Context& ctx, In in, Epi epi, i64 k_max, const i64* d_k, i64* d_
         return;
     }
     i64 nt = ceil_div(k_max, SCAN_TILE);
-    DBuf<i64> partial(ctx, nt), tile_off(ctx, nt);
+    Tmp<i64> partial(ctx, nt), tile_off(ctx, nt);
     k_scan_tile_sums<In><<<(unsigned)nt, SCAN_THREADS, 0, ctx.stream>>>(in, d_k, k_max, partial.p);
     PGGC_LAUNCH_CHECK();
     if (nt == 1) {
@@ -191,11 +191,11 @@ template <class In>
 void det_scan(Context& ctx, In in, double* out, i64 k) {
     if (k <= 0) return;
     i64 groups = ceil_div(k, 32);
-    DBuf<double> tot(ctx, groups);
+    Tmp<double> tot(ctx, groups);
     k_det_scan_groups<In><<<(unsigned)ceil_div(groups * 32, 256), 256, 0, ctx.stream>>>(in, out, k, tot.p);
     PGGC_LAUNCH_CHECK();
     if (groups > 1) {
-        DBuf<double> S(ctx, groups);
+        Tmp<double> S(ctx, groups);
         det_scan(ctx, DArrIn{tot.p}, S.p, groups);
         k_det_scan_add<<<(unsigned)ceil_div(k, 256), 256, 0, ctx.stream>>>(out, k, S.p);
         PGGC_LAUNCH_CHECK();
@@ -229,7 +229,7 @@ void det_reduce(Context& ctx, In in, i64 k, double* d_out) {
         PGGC_LAUNCH_CHECK();
         return;
     }
-    DBuf<double> part(ctx, nb);
+    Tmp<double> part(ctx, nb);
     k_det_reduce_level<In><<<(unsigned)nb, 1024, 0, ctx.stream>>>(in, k, part.p);
     PGGC_LAUNCH_CHECK();
     det_reduce(ctx, DArrIn{part.p}, nb, d_out);
@@ -313,7 +313,7 @@ void radix_sort_pairs(Context& ctx, u64* keys, P* vals, i64 k, int begin_bit, in
                       P* vals_tmp) {
     if (k <= 1) return;
     i64 ntiles = ceil_div(k, RS_TILE);
-    DBuf<i64> hist(ctx, 256 * ntiles);
+    Tmp<i64> hist(ctx, 256 * ntiles);
     u64 *ka = keys, *kb = keys_tmp;
     P *va = vals, *vb = vals_tmp;
     unsigned grid = (unsigned)ceil_div(ntiles, RS_WARPS);

@@ -265,3 +265,33 @@ def test_build_coarse_graph_row_wider_than_shared_table(mem, weighted):
         assert np.array_equal(a, b)
     rg = cg.to_host()[0]
     assert rg[1] - rg[0] == leaves - 1
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_select_pass_vertex_wider_than_shared_table(mem, weighted):
+    """A 40,000-degree hub whose neighbours are all in distinct clusters: more
+    candidate clusters than a 16,384-slot shared table holds, so the hub takes
+    the global-table pass."""
+    leaves = 40000
+    rng = np.random.default_rng(9)
+    w = rng.uniform(0.5, 1.5, leaves).astype(np.float32) if weighted else None
+    hg = G.from_edges(leaves + 1, [(0, i) for i in range(1, leaves + 1)], w)
+    obj = pg.OBJ_WMOD if weighted else pg.OBJ_MOD
+    og, wg = _pair(mem, hg, obj)
+    n = hg.n
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    part = np.arange(n, dtype=np.int32)
+    _, _, _, vw = og.arrays()
+    td = vw.astype(wg.vdtype)
+    pv = np.zeros(n, wg.vdtype)
+    cd_o.set_state(td, 0)
+    cd_g.set_state(n, td, 0)
+    dest0 = np.full(n, pg.NULL_PART, np.int32)
+    gain0 = np.zeros(n, np.float32)
+    for fr in (0.0, 0.75):
+        do, go, ko = O.select(og, cd_o, part, pv, dest0, fr, False, gain=gain0)
+        dg, gg_, kg = pg.select_pass(mem, wg, cd_g, part, pv, dest0, fr, False, gain=gain0)
+        assert ko == kg
+        assert np.array_equal(do, dg)
+        assert np.array_equal(go.view(np.int32), gg_.view(np.int32))
