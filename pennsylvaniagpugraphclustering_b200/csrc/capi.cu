@@ -204,6 +204,7 @@ std::unique_ptr<Graph<W>> make_graph(Context& ctx, int64_t n, int64_t nnz, const
     } else {
         default_vertex_weights<W>(ctx, *g, objective);
     }
+    row_sums<W>(ctx, *g);
     ctx.sync();
     return g;
 }

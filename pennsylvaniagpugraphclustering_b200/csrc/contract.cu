@@ -17,7 +17,7 @@
 //     with a global table for the rows that overflow it; weights are summed
 //     exactly (int64 / FP64);
 //  5. a prefix sum of the unique counts gives the coarse row offsets;
-//  6. each row is sorted by column (warp rank sort, block rank sort in shared
+//  6. each row is sorted by column (warp rank sort, block bitonic sort in shared
 //     memory, LSD radix sort for rows above 4096 entries) and written out.
 // The output is the canonical (row, col)-sorted coarse CSR.
 #include <optional>
@@ -412,45 +412,54 @@ __global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* li
 constexpr int PB_MID = 1024;
 constexpr int PB_MAX = 4096;
 
-// block per row of up to CAP entries: the keys are staged in shared memory and
-// every thread ranks its CAP / THREADS keys against all of them (the keys of a
-// row are distinct), then writes each entry at its rank.  u passes over
-// shared memory (broadcast reads) replace a bitonic network's log^2 barriers.
+// block per row of up to CAP entries: bitonic sort of (key, value) pairs in
+// shared memory, T = next_pow2(u) padded with INT_MAX keys
 template <class W, int THREADS, int CAP>
 __global__ void __launch_bounds__(THREADS) k_place_block(const i32* list, const i64* d_count, const i64* P,
                                                          const i64* cstart, const i64* ucount, const i64* rowptr,
                                                          const i32* skey, const typename Traits<W>::V* sval, i32* col,
                                                          W* wout) {
-    constexpr int PER = CAP / THREADS;
+    using V = typename Traits<W>::V;
     __shared__ i32 kk[CAP];
+    __shared__ V vv[CAP];
     const i64 count = *d_count;
     for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
         const i32 c = list[x];
         const i64 src = P[cstart[c]];
-        const int u = (int)ucount[c];
-        const i64 dst = rowptr[c];
-        for (int s = threadIdx.x; s < u; s += THREADS) kk[s] = skey[src + s];
+        const i64 u = ucount[c];
+        const u32 T = next_pow2_u32((u32)u);
+        for (u32 s = threadIdx.x; s < T; s += THREADS) {
+            kk[s] = s < u ? skey[src + s] : 2147483647;
+            vv[s] = s < u ? sval[src + s] : V(0);
+        }
         __syncthreads();
-        i32 mk[PER];
-        int rk[PER];
-#pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int s = threadIdx.x + q * THREADS;
-            mk[q] = s < u ? kk[s] : 2147483647;
-            rk[q] = 0;
-        }
-        for (int t = 0; t < u; t++) {
-            const i32 o = kk[t];
-#pragma unroll
-            for (int q = 0; q < PER; q++) rk[q] += o < mk[q] ? 1 : 0;
-        }
-#pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int s = threadIdx.x + q * THREADS;
-            if (s < u) {
-                col[dst + rk[q]] = mk[q];
-                wout[dst + rk[q]] = to_w<W>(sval[src + s]);
+        for (u32 k = 2; k <= T; k <<= 1) {
+            for (u32 j = k >> 1; j > 0; j >>= 1) {
+                for (u32 t = threadIdx.x; t < T; t += THREADS) {
+                    const u32 q = t ^ j;
+                    if (q > t) {
+                        const bool up = (t & k) == 0;
+                        const i32 a0 = kk[t], a1 = kk[q];
+                        if ((a0 > a1) == up) {
+                            kk[t] = a1;
+                            kk[q] = a0;
+                            const V v0 = vv[t];
+                            vv[t] = vv[q];
+                            vv[q] = v0;
+                        }
+                    }
+                }
+                // a stride below 32 keeps every pair inside one warp's
+                // 32-aligned slices (THREADS is a multiple of 32), so only the
+                // last step of each merge needs the block barrier
+                if (j >= 32 || j == 1) __syncthreads();
+                else __syncwarp();
             }
+        }
+        const i64 dst = rowptr[c];
+        for (u32 s = threadIdx.x; s < u; s += THREADS) {
+            col[dst + s] = kk[s];
+            wout[dst + s] = to_w<W>(vv[s]);
         }
         __syncthreads();
     }

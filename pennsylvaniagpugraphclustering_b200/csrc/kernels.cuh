@@ -38,6 +38,7 @@ struct Graph {
     DBuf<i32> col;
     DBuf<W> w;
     DBuf<V> vtx_w;
+    mutable DBuf<V> rsum;  // row weight sums, computed on first use by the sweep
     // borrowed (caller-owned) arrays take precedence over the owned ones
     const i64* b_rowptr = nullptr;
     const i32* b_col = nullptr;
@@ -109,6 +110,10 @@ template <class W>
 i64 select_pass(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* part,
                 const typename Traits<W>::V* pvals, ClusterState<typename Traits<W>::V>& cs, i32* dest, float* gain,
                 float filter_ratio, bool initial, bool constrained, const i32* constraint);
+
+// row weight sums of a graph (kept in the graph; computed on first call)
+template <class W>
+const typename Traits<W>::V* row_sums(Context& ctx, const Graph<W>& g);
 
 // own-cluster weight of every vertex under `labels` (canonical sums)
 template <class W>

@@ -498,6 +498,19 @@ __global__ void k_contig_apply(i64 n, const i32* vcmap, const i32* newid, i32* o
         out[u] = newid[vcmap[u]];
 }
 
+// Refinement temporaries live in grow-only workspace slots of the context
+// (sized by the largest level and reused), so the level loop does not go
+// through the allocator for them.
+enum RefineSlot : int {
+    RS_PV = 90, RS_WELL, RS_HN, RS_ORDER, RS_VCMAP, RS_KEYS, RS_KEYS2, RS_IDS, RS_IDS2, RS_CNT, RS_ROWMAP, RS_TS,
+    RS_INNER, RS_OC, RS_INC, RS_BREAK, RS_NEWID, RS_TOT
+};
+template <class T>
+struct RBuf {
+    T* p;
+    RBuf(Context& c, int slot, i64 count) : p(c.ws_get<T>(slot, std::max<i64>(count, 1))) {}
+};
+
 template <class W>
 i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* constraint,
                     const ClusterState<typename Traits<W>::V>& cs, u32 seed_pick, u32 seed_order, i32* vcmap_out) {
@@ -514,12 +527,12 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     const int gw = (int)std::min<i64>(ceil_div(std::max<i64>(nsmall, 1), 8), (i64)ctx.num_sms * 16);
     const int gb = (int)std::min<i64>(std::max<i64>(nmass, 1), (i64)ctx.num_sms * 2);
 
-    DBuf<V> pv(ctx, n);
+    RBuf<V> pv(ctx, RS_PV, n);
     own_weights<W>(ctx, g, ord, constraint, pv.p);
-    DBuf<unsigned char> well(ctx, n);
+    RBuf<unsigned char> well(ctx, RS_WELL, n);
     k_well<W><<<grid, 256, 0, ctx.stream>>>(gv, constraint, pv.p, cs.total_deg.p, gamma, well.p);
     PGGC_LAUNCH_CHECK();
-    DBuf<i32> hn(ctx, n), order(ctx, n), vcmap(ctx, n);
+    RBuf<i32> hn(ctx, RS_HN, n), order(ctx, RS_ORDER, n), vcmap(ctx, RS_VCMAP, n);
     PickArgs<W> pa{gv, constraint, well.p, gamma, seed_pick, hn.p};
     if (g.uniform) {
         if (nsmall > 0) {
@@ -559,21 +572,21 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     PGGC_LAUNCH_CHECK();
 
     // --- gamma connectivity
-    DBuf<u64> keys(ctx, n), keys2(ctx, n);
-    DBuf<i32> ids(ctx, n), ids2(ctx, n);
+    RBuf<u64> keys(ctx, RS_KEYS, n), keys2(ctx, RS_KEYS2, n);
+    RBuf<i32> ids(ctx, RS_IDS, n), ids2(ctx, RS_IDS2, n);
     k_sort_keys<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, order.p, keys.p, ids.p);
     PGGC_LAUNCH_CHECK();
     radix_sort_pairs<i32>(ctx, keys.p, ids.p, n, 0, 31 + bits_for((u64)(n - 1)), keys2.p, ids2.p);
-    DBuf<i64> cnt(ctx, n + 1), row_map(ctx, n + 1);
+    RBuf<i64> cnt(ctx, RS_CNT, n + 1), row_map(ctx, RS_ROWMAP, n + 1);
     PGGC_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(i64) * (n + 1), ctx.stream));
     k_hist<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, cnt.p);
     PGGC_LAUNCH_CHECK();
     scan_apply(ctx, ArrIn{cnt.p}, ArrOutExcl{row_map.p}, n + 1, nullptr, nullptr);
-    DBuf<V> ts(ctx, n), inner(ctx, n), oc(ctx, n);
+    RBuf<V> ts(ctx, RS_TS, n), inner(ctx, RS_INNER, n), oc(ctx, RS_OC, n);
     if constexpr (std::is_same<V, i64>::value) {
         scan_apply(ctx, TsIn<i64>{ids.p, g.vtx_w.p, n}, ArrOutExcl{ts.p}, n, nullptr, nullptr);
     } else {
-        DBuf<double> inc(ctx, n);
+        RBuf<double> inc(ctx, RS_INC, n);
         det_scan(ctx, TsIn<double>{ids.p, g.vtx_w.p, n}, inc.p, n);
         k_shift_excl<<<grid, 256, 0, ctx.stream>>>(n, inc.p, ts.p);
         PGGC_LAUNCH_CHECK();
@@ -586,7 +599,7 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
         k_inner_block<W><<<gb, 1024, 0, ctx.stream>>>(gv, mass_list, nmass, vcmap.p, order.p, inner.p);
         PGGC_LAUNCH_CHECK();
     }
-    DBuf<long long> breakers(ctx, n);
+    RBuf<long long> breakers(ctx, RS_BREAK, n);
     fill<long long>(ctx, breakers.p, n, (long long)n);
     GammaArgs<W> ga{n, ids.p, vcmap.p, row_map.p, ts.p, inner.p, oc.p, g.vtx_w.p, cs.total_deg.p, constraint, gamma,
                     breakers.p};
@@ -595,7 +608,7 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     if constexpr (std::is_same<V, i64>::value) {
         scan_apply(ctx, OcInI<i64>{ids.p, pv.p, inner.p}, OcEpiI{ids.p, oc.p}, n, nullptr, nullptr);
     } else {
-        DBuf<double> inc(ctx, n);
+        RBuf<double> inc(ctx, RS_INC, n);
         det_scan(ctx, OcInD{ids.p, pv.p, inner.p}, inc.p, n);
         k_scatter_by_ids<<<grid, 256, 0, ctx.stream>>>(n, ids.p, inc.p, oc.p);
         PGGC_LAUNCH_CHECK();
@@ -606,8 +619,8 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     PGGC_LAUNCH_CHECK();
 
     // --- contigitize
-    DBuf<i32> newid(ctx, n);
-    DBuf<i64> tot(ctx, 1);
+    RBuf<i32> newid(ctx, RS_NEWID, n);
+    RBuf<i64> tot(ctx, RS_TOT, 1);
     scan_apply(ctx, RootFlag{vcmap.p}, RootEpi{newid.p}, n, nullptr, tot.p);
     k_contig_apply<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, newid.p, vcmap_out);
     PGGC_LAUNCH_CHECK();

@@ -17,6 +17,7 @@
 //    cluster ids and the strict prefix follow the reference's move order.
 //  * One host round trip per sweep (candidate and move counts); everything else
 //    reads counts from device memory.
+#include <mutex>
 #include "kernels.cuh"
 #include "filter.cuh"
 
@@ -95,6 +96,7 @@ struct SelArgs {
     const V* td;
     const i32* constraint;
     const i64* label_count;  // device
+    const V* rsum;           // row weight sums (NULL: no bound check)
     float pm;
     float fr;
     int initial;
@@ -128,6 +130,18 @@ __device__ __forceinline__ VCtx sel_prologue(const SelArgs<W>& a, i32 i) {
     v.p_conn = to_f(a.pvals[i]) - to_f(V(a.td[v.p] - w)) * v.multi;
     v.thr = v.p_conn < 0.0f ? 0.0f : (float)((double)v.p_conn * (1.0 - (double)a.fr));
     return v;
+}
+
+// Exact skip: no neighbour cluster can carry more weight than the vertex's
+// weight outside its own cluster, ext = rowsum - pval; when even ext rounds
+// (one FP32 step up, covering FP64 rounding in either sum) below the
+// candidate threshold, no cluster passes the `f >= thr` test of sel_eval and
+// the edges need not be read: the outcome is the no-candidate outcome.
+template <class W>
+__device__ __forceinline__ bool sel_no_candidate(const SelArgs<W>& a, i32 i, const VCtx& vc) {
+    if (!a.rsum || a.initial) return false;
+    const float fe = nextafterf(to_f(a.rsum[i] - a.pvals[i]), INFINITY);
+    return !(fe >= vc.thr);
 }
 
 template <class W, bool CON>
@@ -282,6 +296,7 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, R
         }
         VCtx vc = sel_prologue(a, i);
         i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        if (sel_no_candidate(a, i, vc)) e = b;
         pb += sel_bytes(a, e - b, true);
         Best best = none_best();
         if (a.initial) {
@@ -451,7 +466,7 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
             if (act[u]) {
                 vc[u] = sel_prologue(a, iv[u]);
                 b[u] = a.g.rowptr[iv[u]];
-                e[u] = a.g.rowptr[iv[u] + 1];
+                e[u] = sel_no_candidate(a, iv[u], vc[u]) ? b[u] : a.g.rowptr[iv[u] + 1];
             }
             if (r == 0 && iv[u] >= 0) pb += sel_bytes(a, e[u] - b[u], act[u]);
         }
@@ -525,6 +540,7 @@ __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg
             continue;
         }
         VCtx vc = sel_prologue(a, i);
+        if (sel_no_candidate(a, i, vc)) e = b;
         Best best = none_best();
         if (a.initial) {
             for (i64 j = b + threadIdx.x; j < e; j += THREADS)
@@ -1371,6 +1387,34 @@ inline int grid_for(Context& ctx, i64 work, int per_block, int max_per_sm = 16) 
     return (int)std::max<i64>(1, std::min<i64>(ceil_div(std::max<i64>(work, 1), per_block), (i64)ctx.num_sms * max_per_sm));
 }
 
+// Row weight sums (one thread per vertex; computed once per graph)
+template <class W>
+__global__ void k_row_sums(DGraph<W> g, typename Traits<W>::V* out) {
+    using V = typename Traits<W>::V;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < g.n; i += (i64)gridDim.x * blockDim.x) {
+        V s = V(0);
+        for (i64 j = g.rowptr[i]; j < g.rowptr[i + 1]; j++) s += V(g.wgt(j));
+        out[i] = s;
+    }
+}
+
+template <class W>
+const typename Traits<W>::V* row_sums(Context& ctx, const Graph<W>& g) {
+    using V = typename Traits<W>::V;
+    if (g.n == 0) return nullptr;
+    // graphs are created with their sums (make_graph) or by one context
+    // (coarse levels); the lock covers a graph first used by several threads
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!g.rsum.p) {
+        g.rsum = DBuf<V>(ctx, g.n);
+        int grid = (int)std::min<i64>(ceil_div(g.n, 256), (i64)ctx.num_sms * 16);
+        k_row_sums<W><<<grid, 256, 0, ctx.stream>>>(g.view(), g.rsum.p);
+        PGGC_LAUNCH_CHECK();
+    }
+    return g.rsum.p;
+}
+
 template <class W>
 struct Mover {
     using V = typename Traits<W>::V;
@@ -1502,6 +1546,7 @@ struct Mover {
         a.td = td;
         a.constraint = constraint;
         a.label_count = lcount;
+        a.rsum = row_sums<W>(ctx, g);
         a.pm = pm;
         a.fr = fr;
         a.initial = initial ? 1 : 0;
@@ -1893,7 +1938,8 @@ i64 select_pass(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32*
                                 bool, i32*, bool, bool, int, MoveStats*);                                           \
     template i64 select_pass<W>(Context&, const Graph<W>&, const Ordering&, const i32*, const Traits<W>::V*,         \
                                 ClusterState<Traits<W>::V>&, i32*, float*, float, bool, bool, const i32*);          \
-    template void own_weights<W>(Context&, const Graph<W>&, const Ordering&, const i32*, Traits<W>::V*);
+    template void own_weights<W>(Context&, const Graph<W>&, const Ordering&, const i32*, Traits<W>::V*);          \
+    template const Traits<W>::V* row_sums<W>(Context&, const Graph<W>&);
 PGGC_INST_LM(i32)
 PGGC_INST_LM(float)
 
