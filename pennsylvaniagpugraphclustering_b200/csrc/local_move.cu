@@ -45,14 +45,23 @@ struct Best {
 };
 __device__ __forceinline__ bool better(float jc, i32 c, const Best& b) { return jc > b.jc || (jc == b.jc && c < b.c); }
 __device__ __forceinline__ Best none_best() { return Best{-INFINITY, 2147483647}; }
-__device__ __forceinline__ void warp_best(Best& b) {
-#pragma unroll
-    for (int d = 16; d >= 1; d >>= 1) {
-        float oj = __shfl_xor_sync(FULL, b.jc, d);
-        i32 oc = __shfl_xor_sync(FULL, b.c, d);
-        if (better(oj, oc, b)) b = Best{oj, oc};
-    }
+// Order-preserving map of a float onto u32 (no NaN here); with it the best
+// (largest gain, then smallest cluster id) of a lane group is two hardware
+// reductions instead of a shuffle butterfly.  Gains are never -0.0 (a
+// candidate has f > 0 and f - x is +0.0 when equal), so float equality and
+// key equality agree.
+__device__ __forceinline__ u32 f2ord(float f) {
+    const u32 b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
+__device__ __forceinline__ float ord2f(u32 k) { return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k); }
+__device__ __forceinline__ void reduce_best(Best& b, unsigned mask) {
+    const u32 k = f2ord(b.jc);
+    const u32 mk = __reduce_max_sync(mask, k);
+    const u32 mc = __reduce_min_sync(mask, k == mk ? (u32)b.c : 0xFFFFFFFFu);
+    b = Best{ord2f(mk), (i32)mc};
+}
+__device__ __forceinline__ void warp_best(Best& b) { reduce_best(b, FULL); }
 
 // A slice of a vertex list whose bounds live on the host or in device memory.
 struct Range {
@@ -97,6 +106,7 @@ struct SelArgs {
     const i32* constraint;
     const i64* label_count;  // device
     const V* rsum;           // row weight sums (NULL: no bound check)
+    int keys32;              // cluster ids < 2^29: group match keys fit 32 bits
     float pm;
     float fr;
     int initial;
@@ -425,12 +435,8 @@ inline void build_class_lists(Context& ctx, const i64* rowptr, const Ordering& o
 
 template <int G>
 __device__ __forceinline__ void group_best(Best& b) {
-#pragma unroll
-    for (int d = G / 2; d >= 1; d >>= 1) {
-        float oj = __shfl_xor_sync(FULL, b.jc, d);
-        i32 oc = __shfl_xor_sync(FULL, b.c, d);
-        if (better(oj, oc, b)) b = Best{oj, oc};
-    }
+    const unsigned mask = G == 32 ? FULL : (((1u << G) - 1u) << (lane_id() & ~(G - 1)));
+    reduce_best(b, mask);
 }
 
 // G-lane groups, one vertex each, for vertices of degree <= G (single chunk):
@@ -495,8 +501,16 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
             for (int u = 0; u < UV; u++) {
                 Best best = none_best();
                 const bool keep = c[u] >= 0 && c[u] != vc[u].p;
-                u64 key = keep ? (((u64)grp << 32) | (u64)(u32)c[u]) : (0xFFFFFFFF00000000ull | (u64)l);
-                unsigned peers = __match_any_sync(FULL, key);
+                unsigned peers;
+                if (a.keys32) {
+                    // bit 31 marks lanes without a candidate (unique per lane),
+                    // bits 29-30 the group
+                    const u32 key = keep ? (((u32)grp << 29) | (u32)c[u]) : (0x80000000u | (u32)l);
+                    peers = __match_any_sync(FULL, key);
+                } else {
+                    const u64 key = keep ? (((u64)grp << 32) | (u64)(u32)c[u]) : (0xFFFFFFFF00000000ull | (u64)l);
+                    peers = __match_any_sync(FULL, key);
+                }
                 bool leader = keep && ((peers & lanemask_lt()) == 0);
                 V sum = a.g.w ? group_sum<V>(peers, wv[u], leader) : V(__popc(peers));
                 if (leader) sel_eval<W, CON>(a, vc[u], c[u], sum, best);
@@ -1553,6 +1567,7 @@ struct Mover {
         a.err = ctx.d_err;
         a.prof = nullptr;
         a.probe_cap = ctx.probe_cap;
+        a.keys32 = cap < ((i64)1 << 29) ? 1 : 0;
         return a;
     }
 
