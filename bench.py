@@ -146,6 +146,7 @@ def cpu_run(sample_n: int, seed: int, steps: int, warmup: int):
         q = st.objective
     sec = statistics.mean(times)
     return {"value": g.m / sec, "unit": UNIT, "cores": int(O.lib().orc_num_threads()), "kind": "port",
+            "ms_per_run": sec * 1000.0,
             "sample": f"DC-SBM n={sample_n} (m={g.m}) with the workload's parameters, seed {seed}; "
                       f"pLeiden+ until stable; {steps} timed runs, mean {sec:.3f} s; modularity {q:.6f}"}
 
@@ -156,7 +157,7 @@ def reference_arm(args):
         return
     res = cpu_run(args.cpu_sample_n, args.seed, args.steps, args.warmup)
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_run"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "sample_n": args.cpu_sample_n},
             "cpu_baseline": res,
