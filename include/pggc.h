@@ -205,6 +205,34 @@ typedef struct pggc_batch_job {
 } pggc_batch_job;
 pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, int streams);
 
+/* ---- memetic driver (app/memetic_clustering.cpp:27-219) -------------------
+ * meme_cluster: pop_size pLeiden+ clusterings, then offspring from the
+ * intersection of two tournament-selected parents, refined by constrained
+ * pLouvain and five pLeiden+ improvement passes, each replacing the most
+ * similar (cut-edge signature) worse member.  The reference runs for a wall
+ * time; here the loop stops after `offspring` children (< 0: no limit) or
+ * `time_limit_s` seconds (<= 0: no limit), whichever comes first (at least one
+ * limit must be set).  `seed` replaces std::random_device.  labels_out gets the
+ * best member (n int32). */
+typedef struct pggc_meme_stats {
+    double objective;    /* best member's objective */
+    int64_t label_count;
+    int64_t offspring;   /* children made */
+    int64_t replaced;    /* children that entered the population */
+    double best_initial; /* best objective of the initial population */
+} pggc_meme_stats;
+pggc_status pggc_meme_cluster(pggc_context* ctx, const pggc_graph* g, int objective, double lambda_mult, int pop_size,
+                              int64_t offspring, double time_limit_s, uint64_t seed, int32_t* labels_out,
+                              int mem_kind, pggc_meme_stats* stats);
+/* intersection_cluster (:27-62): out[i] = rank of (c1[i], c2[i]) among the
+ * distinct pairs in ascending order (labels in [0, n)); *count_out = pairs */
+pggc_status pggc_intersect_clusters(pggc_context* ctx, const int32_t* c1, const int32_t* c2, int64_t n, int32_t* out,
+                                    int64_t* count_out, int mem_kind);
+/* gen_signature (:64-104): bit j of sign_out (ceil(nnz / 32) words) is set when
+ * edge j joins two clusters */
+pggc_status pggc_cut_signature(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, uint32_t* sign_out,
+                               int mem_kind);
+
 /* verify_objective<uniform> (app/verify_objective.cpp:64-89) in int64 / FP64 */
 pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, int objective,
                                   double lambda_mult, int mem_kind, double* objective_out, double* raw_obj_out);

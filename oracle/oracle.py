@@ -76,8 +76,18 @@ def lib():
         L.orc_murmur3.argtypes = [u32]
         L.orc_murmur3.restype = u32
         L.orc_num_threads.restype = ci
+        L.orc_intersect.argtypes = [vp, vp, i64, vp]
+        L.orc_intersect.restype = i64
+        L.orc_signature.argtypes = [vp, vp, vp]
+        L.orc_meme_cluster.argtypes = [vp, ci, dbl, ci, i64, u64, vp, ctypes.POINTER(MemeStats)]
+        L.orc_meme_cluster.restype = ci
         _LIB = L
     return _LIB
+
+
+class MemeStats(ctypes.Structure):
+    _fields_ = [("objective", ctypes.c_double), ("label_count", ctypes.c_int64), ("offspring", ctypes.c_int64),
+                ("replaced", ctypes.c_int64), ("best_initial", ctypes.c_double)]
 
 
 def _p(a):
@@ -244,3 +254,27 @@ def det_reduce(a) -> float:
 
 def murmur3(k: int) -> int:
     return int(lib().orc_murmur3(k & 0xFFFFFFFF))
+
+
+# ---- memetic driver (app/memetic_clustering.cpp:27-219) -----------------------
+def intersect(c1, c2):
+    """intersection_cluster with canonical ids (ranks of the sorted distinct pairs)."""
+    a = np.ascontiguousarray(c1, np.int32)
+    b = np.ascontiguousarray(c2, np.int32)
+    out = np.empty(len(a), np.int32)
+    k = lib().orc_intersect(_p(a), _p(b), len(a), _p(out))
+    return out, k
+
+
+def signature(g: Graph, labels):
+    lab = np.ascontiguousarray(labels, np.int32)
+    out = np.empty(max((g.nnz + 31) // 32, 1), np.uint32)
+    lib().orc_signature(g.h, _p(lab), _p(out))
+    return out
+
+
+def meme_cluster(g: Graph, objective, lambda_mult=1.0, pop_size=8, offspring=16, seed=1):
+    out = np.empty(g.n, np.int32)
+    st = MemeStats()
+    lib().orc_meme_cluster(g.h, objective, float(lambda_mult), pop_size, offspring, seed, _p(out), ctypes.byref(st))
+    return out, st

@@ -219,6 +219,7 @@ template <> struct Traits<float> { using V = double; };
 template <class W>
 struct Graph {
     using V = typename Traits<W>::V;
+    using Weight = W;
     i64 n = 0, nnz = 0;
     std::vector<i64> rowptr;
     std::vector<i32> col;
@@ -1612,6 +1613,143 @@ int orc_louvain_part(void* gh, void* cdh, int constrained, const int32_t* constr
     }
     Engine<i32> e;
     return run(e, g->gi, cd->ci);
+}
+
+// ---- memetic driver, app/memetic_clustering.cpp:27-219 ---------------------
+// intersection_cluster (:27-62) with canonical ids: ranks of the distinct
+// (c1, c2) pairs in ascending order (the reference's ids follow hash-slot order)
+int64_t orc_intersect(const int32_t* c1, const int32_t* c2, int64_t n, int32_t* out) {
+    std::vector<std::pair<u64, i32>> kv((size_t)n);
+    for (int64_t i = 0; i < n; i++) kv[i] = {((u64)(u32)c1[i] << 32) | (u64)(u32)c2[i], (i32)i};
+    std::sort(kv.begin(), kv.end());
+    int64_t r = -1;
+    for (int64_t x = 0; x < n; x++) {
+        if (x == 0 || kv[x].first != kv[x - 1].first) r++;
+        out[kv[x].second] = (i32)r;
+    }
+    return r + 1;
+}
+
+// gen_signature (:64-104): bit j set when edge j joins two clusters
+void orc_signature(void* gh, const int32_t* labels, uint32_t* sign) {
+    auto* g = (OrcGraph*)gh;
+    auto run = [&](auto& gg) {
+        const int64_t words = (std::max<int64_t>(gg.nnz, 1) + 31) / 32;
+        std::fill(sign, sign + words, 0u);
+        for (int64_t i = 0; i < gg.n; i++)
+            for (int64_t j = gg.rowptr[i]; j < gg.rowptr[i + 1]; j++)
+                if (labels[i] != labels[gg.col[j]]) sign[j / 32] |= 1u << (j % 32);
+    };
+    if (g->kind == 2) run(g->gf);
+    else run(g->gi);
+}
+
+struct OrcMemeStats {
+    double objective;
+    int64_t label_count;
+    int64_t offspring;
+    int64_t replaced;
+    double best_initial;
+};
+
+static inline int64_t orc_uniform_below(SplitMix64& r, int64_t m) {
+    return (int64_t)(((unsigned __int128)r.next() * (u64)m) >> 64);
+}
+
+// meme_cluster (:118-219) with `offspring` children instead of the time limit;
+// the random stream matches the GPU driver's call for call
+int orc_meme_cluster(void* gh, int objective, double mult, int pop_size, int64_t offspring, uint64_t seed,
+                     int32_t* labels_out, OrcMemeStats* st) {
+    auto* g = (OrcGraph*)gh;
+    auto run = [&](auto& eng, auto& gg) {
+        using W = typename std::remove_reference_t<decltype(gg)>::Weight;
+        const int64_t n = gg.n;
+        const int64_t words = (std::max<int64_t>(gg.nnz, 1) + 31) / 32;
+        struct Member {
+            std::vector<i32> clusters;
+            std::vector<uint32_t> sign;
+            double obj = 0;
+            int64_t labels = 0;
+        };
+        std::vector<Member> pop((size_t)pop_size);
+        SplitMix64 rng(seed);
+        double best_initial = -std::numeric_limits<double>::infinity();
+        auto signature = [&](const std::vector<i32>& c, std::vector<uint32_t>& s) {
+            s.assign((size_t)words, 0u);
+            for (int64_t i = 0; i < n; i++)
+                for (int64_t j = gg.rowptr[i]; j < gg.rowptr[i + 1]; j++)
+                    if (c[i] != c[gg.col[j]]) s[j / 32] |= 1u << (j % 32);
+        };
+        i64 lv = 0, tn = 0;
+        for (int p = 0; p < pop_size; p++) {
+            auto cd = make_objective<W>(gg, objective, mult);
+            pop[p].clusters = eng.leiden_part(gg, cd, true, false, nullptr, rng.next(), &lv, &tn);
+            pop[p].obj = cd.get_objective();
+            pop[p].labels = cd.label_count;
+            signature(pop[p].clusters, pop[p].sign);
+            best_initial = std::max(best_initial, pop[p].obj);
+        }
+        auto pick = [&]() {
+            const int64_t a = orc_uniform_below(rng, pop_size);
+            const int64_t b = (a + orc_uniform_below(rng, pop_size - 1)) % pop_size;
+            return pop[a].obj > pop[b].obj ? a : b;
+        };
+        int64_t made = 0, replaced = 0;
+        std::vector<i32> constraint((size_t)n);
+        std::vector<uint32_t> csign;
+        while (made < offspring) {
+            const int64_t p1 = pick();
+            int64_t p2 = p1;
+            while (p2 == p1) p2 = pick();
+            orc_intersect(pop[p1].clusters.data(), pop[p2].clusters.data(), n, constraint.data());
+            auto cd = make_objective<W>(gg, objective, mult);
+            std::vector<i32> child = eng.louvain_part(gg, cd, true, constraint, &lv, &tn);
+            for (int x = 0; x < 5; x++) {
+                std::vector<i32> in = child;
+                child = eng.leiden_part(gg, cd, true, true, in.data(), rng.next(), &lv, &tn);
+            }
+            made++;
+            const double obj = cd.get_objective();
+            signature(child, csign);
+            int64_t am = -1;
+            int64_t min_diff = std::numeric_limits<int64_t>::max();
+            for (int p = 0; p < pop_size; p++) {
+                if (pop[p].obj < obj) {
+                    int64_t d = 0;
+                    for (int64_t w = 0; w < words; w++) d += __builtin_popcount(csign[w] ^ pop[p].sign[w]);
+                    if (d < min_diff) {
+                        min_diff = d;
+                        am = p;
+                    }
+                }
+            }
+            if (am >= 0) {
+                pop[am].clusters = child;
+                pop[am].sign = csign;
+                pop[am].obj = obj;
+                pop[am].labels = cd.label_count;
+                replaced++;
+            }
+        }
+        int am = 0;
+        for (int p = 1; p < pop_size; p++)
+            if (pop[p].obj > pop[am].obj) am = p;
+        std::copy(pop[am].clusters.begin(), pop[am].clusters.end(), labels_out);
+        if (st) {
+            st->objective = pop[am].obj;
+            st->label_count = pop[am].labels;
+            st->offspring = made;
+            st->replaced = replaced;
+            st->best_initial = best_initial;
+        }
+        return 0;
+    };
+    if (g->kind == 2) {
+        Engine<float> e;
+        return run(e, g->gf);
+    }
+    Engine<i32> e;
+    return run(e, g->gi);
 }
 
 double orc_verify_objective(void* gh, const int32_t* labels, int objective, double mult, double* raw_obj) {

@@ -6,7 +6,7 @@ is hand-written CUDA in ``csrc/`` behind the C ABI of ``include/pggc.h``.
 :mod:`.api` mirrors the reference's host interface on top of that ABI.
 """
 from .api import (NEW_PART, NO_MOVE, NULL_PART, OBJECTIVES, batch_run, build_coarse_graph, cluster_data,
-                  clustering_methods,
+                  clustering_methods, cut_signature, intersect_clusters, meme_cluster,
                   coarsen_leidenR, constant_potts, generate_orderings, get_objective, local_move, local_move_strict,
                   memory_store, modularity, normalized_lcc, run_clustering, select_pass, verify_objective,
                   weighted_graph)

@@ -49,6 +49,14 @@ class BatchJob(ctypes.Structure):
                 ("status", ctypes.c_int)]
 
 
+class MemeStats(ctypes.Structure):
+    _fields_ = [("objective", ctypes.c_double), ("label_count", ctypes.c_int64), ("offspring", ctypes.c_int64),
+                ("replaced", ctypes.c_int64), ("best_initial", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 # name -> (restype, argtypes)
 _vp, _i64, _ci, _dbl, _u32, _u64, _flt = (ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float)
@@ -85,6 +93,9 @@ _SIGS = {
     "pggc_filter_enable": (_ci, [_vp, _vp, _flt]),
     "pggc_filter_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _ci]),
     "pggc_batch_run": (_ci, [_vp, _vp, _i64, _ci]),
+    "pggc_meme_cluster": (_ci, [_vp, _vp, _ci, _dbl, _ci, _i64, _dbl, _u64, _vp, _ci, ctypes.POINTER(MemeStats)]),
+    "pggc_intersect_clusters": (_ci, [_vp, _vp, _vp, _i64, _vp, ctypes.POINTER(_i64), _ci]),
+    "pggc_cut_signature": (_ci, [_vp, _vp, _vp, _vp, _ci]),
     "pggc_local_move": (_ci, [_vp, _vp, _vp, _vp, _ci, _ci, _vp, _i64, _ci, _ci, _ci, _ci, ctypes.POINTER(Stats)]),
     "pggc_select_pass": (_ci, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _flt, _ci, _ci, _vp, _ci, ctypes.POINTER(_i64)]),
     "pggc_build_coarse_graph": (_ci, [_vp, _vp, _vp, _i64, _ci, _PP]),

@@ -421,3 +421,33 @@ def batch_run(mem: memory_store, jobs, streams: int = 8):
         arr[k].mem_kind = MEM_HOST
     check(L.lib().pggc_batch_run(mem.handle, ctypes.cast(arr, ctypes.c_void_p), len(jobs), int(streams)))
     return [(outs[k][:jobs[k]["graph"].n], _stats_dict(arr[k].stats)) for k in range(len(jobs))]
+
+
+def meme_cluster(mem: memory_store, g: weighted_graph, objective=None, lambda_mult: float = 1.0, pop_size: int = 8,
+                 offspring: int = 16, time_limit_s: float = 0.0, seed: int = 1):
+    """Memetic clustering (app/memetic_clustering.cpp:118-219); returns (labels, stats dict)."""
+    obj = g.objective if objective is None else objective
+    lab = np.empty(max(g.n, 1), np.int32)
+    st = L.MemeStats()
+    check(L.lib().pggc_meme_cluster(mem.handle, g.handle, int(obj), float(lambda_mult), int(pop_size), int(offspring),
+                                    float(time_limit_s), int(seed), lab.ctypes.data, MEM_HOST, ctypes.byref(st)))
+    return lab[:g.n], st.as_dict()
+
+
+def intersect_clusters(mem: memory_store, c1, c2):
+    """intersection_cluster (app/memetic_clustering.cpp:27-62): (labels, count)."""
+    a = np.ascontiguousarray(c1, np.int32)
+    b = np.ascontiguousarray(c2, np.int32)
+    out = np.empty(max(len(a), 1), np.int32)
+    k = ctypes.c_int64()
+    check(L.lib().pggc_intersect_clusters(mem.handle, a.ctypes.data, b.ctypes.data, len(a), out.ctypes.data,
+                                          ctypes.byref(k), MEM_HOST))
+    return out[:len(a)], k.value
+
+
+def cut_signature(mem: memory_store, g: weighted_graph, labels):
+    """gen_signature (app/memetic_clustering.cpp:64-104): uint32 words, bit j = edge j is cut."""
+    lab = np.ascontiguousarray(labels, np.int32)
+    out = np.empty(max((g.nnz + 31) // 32, 1), np.uint32)
+    check(L.lib().pggc_cut_signature(mem.handle, g.handle, lab.ctypes.data, out.ctypes.data, MEM_HOST))
+    return out

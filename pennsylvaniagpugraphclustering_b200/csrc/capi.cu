@@ -778,6 +778,73 @@ pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t coun
     });
 }
 
+pggc_status pggc_meme_cluster(pggc_context* ctx, const pggc_graph* g, int objective, double lambda_mult, int pop_size,
+                              int64_t offspring, double time_limit_s, uint64_t seed, int32_t* labels_out,
+                              int mem_kind, pggc_meme_stats* stats) {
+    return guarded([&] {
+        need(ctx && g && labels_out, "NULL argument");
+        need(pop_size >= 2, "pop_size must be at least 2");
+        need(offspring >= 0 || time_limit_s > 0, "set an offspring count or a time limit");
+        need(objective >= PGGC_OBJ_MOD && objective <= PGGC_OBJ_LCC, "unknown objective");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
+            Out<i32> lab(c, labels_out, gr.n, mem_kind, false);
+            MemeStats ms;
+            meme_cluster<W>(c, gr, objective, lambda_mult, pop_size, offspring, time_limit_s, seed, lab.p, &ms);
+            lab.finish();
+            c.sync();
+            if (stats) {
+                stats->objective = ms.objective;
+                stats->label_count = ms.label_count;
+                stats->offspring = ms.offspring;
+                stats->replaced = ms.replaced;
+                stats->best_initial = ms.best_initial;
+            }
+        });
+    });
+}
+
+pggc_status pggc_intersect_clusters(pggc_context* ctx, const int32_t* c1, const int32_t* c2, int64_t n, int32_t* out,
+                                    int64_t* count_out, int mem_kind) {
+    return guarded([&] {
+        need(ctx && (n == 0 || (c1 && c2 && out)), "NULL argument");
+        need(n >= 0, "n must be >= 0");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        In<i32> a(c, c1, n, mem_kind), b(c, c2, n, mem_kind);
+        check_labels(c, a.p, n, std::max<i64>(n, 1), "labels must lie in [0, n)");
+        check_labels(c, b.p, n, std::max<i64>(n, 1), "labels must lie in [0, n)");
+        Out<i32> o(c, out, n, mem_kind, false);
+        const i64 k = intersect_clusters(c, a.p, b.p, n, o.p);
+        o.finish();
+        c.sync();
+        if (count_out) *count_out = k;
+    });
+}
+
+pggc_status pggc_cut_signature(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, uint32_t* sign_out,
+                               int mem_kind) {
+    return guarded([&] {
+        need(ctx && g && labels && sign_out, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        dispatch(g, [&](auto& gr, auto* vtag) {
+            using V = std::remove_pointer_t<decltype(vtag)>;
+            using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
+            In<i32> lab(c, labels, gr.n, mem_kind);
+            check_labels(c, lab.p, gr.n, std::max<i64>(gr.n, 1), "labels must lie in [0, n)");
+            const i64 words = ceil_div(std::max<i64>(gr.nnz, 1), 32);
+            Out<u32> o(c, sign_out, words, mem_kind, false);
+            cut_signature<W>(c, gr, lab.p, o.p);
+            o.finish();
+            c.sync();
+        });
+    });
+}
+
 pggc_status pggc_verify_objective(pggc_context* ctx, const pggc_graph* g, const int32_t* labels, int objective,
                                   double lambda_mult, int mem_kind, double* objective_out, double* raw_obj_out) {
     return guarded([&] {

@@ -156,4 +156,24 @@ template <class W>
 void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool constrained,
                   const i32* constraint, i32* labels_out, RunStats* st);
 
+// ---------------------------------------------------------------------------
+// memetic driver (app/memetic_clustering.cpp:27-219)
+// ---------------------------------------------------------------------------
+struct MemeStats {
+    double objective = 0;
+    i64 label_count = 0;
+    i64 offspring = 0;
+    i64 replaced = 0;
+    double best_initial = 0;
+};
+// ranks of the distinct (c1[i], c2[i]) pairs in ascending order; returns their count
+i64 intersect_clusters(Context& ctx, const i32* c1, const i32* c2, i64 n, i32* out);
+// one bit per directed edge: set when its ends are in different clusters
+template <class W>
+void cut_signature(Context& ctx, const Graph<W>& g, const i32* labels, u32* sign);
+// offspring < 0: no count limit; time_limit_s <= 0: no time limit
+template <class W>
+void meme_cluster(Context& ctx, const Graph<W>& g, int objective, double lambda_mult, int pop_size, i64 offspring,
+                  double time_limit_s, u64 seed, i32* labels_out, MemeStats* st);
+
 }  // namespace pggc
