@@ -95,6 +95,24 @@ pggc_status pggc_context_stream(pggc_context* ctx, void** stream_out);
 pggc_status pggc_graph_create(pggc_context* ctx, int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col,
                               const void* weights, int weight_kind, const void* vtx_w, int objective, int mem_kind,
                               pggc_graph** out);
+/* ---- graph input (app/io/io_mtx.cpp:95-345, app/io/io_metis.cpp:64-181) ---
+ * pggc_graph_load replaces load_graph(g, uniform_ew, fname)
+ * (app/io/io_mtx.cpp:336-345): a path ending in ".mtx" is read as a Matrix
+ * Market coordinate file, anything else as a METIS file.  Mod and CPM ignore
+ * file weights (uses_edge_weights, app/objective_helpers.hpp:24-29); real
+ * weights and weights of non-symmetric files are ignored as in the
+ * reference; pattern files have unit weights.  *edge_uniform_out (may be
+ * NULL) receives the reference's uniform_ew.  Malformed files, METIS vertex
+ * weights and non-square matrices return PGGC_ERR_INVALID.
+ * pggc_graph_from_edges replaces construct_from_edgelist (io_mtx.cpp:95-201)
+ * for 0-based edge lists: self loops and zero weights dropped, both
+ * directions stored, unordered duplicates removed unless `symmetric`, rows
+ * sorted by column.  weights (may be NULL) only with symmetric != 0. */
+pggc_status pggc_graph_load(pggc_context* ctx, const char* path, int objective, int* edge_uniform_out,
+                            pggc_graph** out);
+pggc_status pggc_graph_from_edges(pggc_context* ctx, int64_t n, int64_t m, const int32_t* src, const int32_t* dst,
+                                  const int32_t* weights, int symmetric, int objective, int mem_kind,
+                                  pggc_graph** out);
 pggc_status pggc_graph_destroy(pggc_graph* g);
 pggc_status pggc_graph_dims(const pggc_graph* g, int64_t* n, int64_t* nnz, int* weight_kind);
 /* copies out any non-NULL array (weights only for non-uniform graphs) */

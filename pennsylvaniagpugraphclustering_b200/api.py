@@ -20,6 +20,7 @@ ABI of ``libpggc_b200.so``; there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Optional
 
 import numpy as np
@@ -178,6 +179,39 @@ class weighted_graph:
             self.close()
         except Exception:
             pass
+
+
+def load_graph(mem: memory_store, path, objective: int = OBJ_MOD) -> weighted_graph:
+    """Reads a Matrix Market (``.mtx``) or METIS file into a device graph
+    (load_graph, app/io/io_mtx.cpp:336-345; load_mtx_graph :204-333;
+    load_metis_graph, app/io/io_metis.cpp:64-181).
+
+    Mod and CPM ignore file weights; ``wg.edge_uniform`` is the reference's
+    ``uniform_ew`` after loading.  Malformed files raise ``PggcError``.
+    """
+    h = ctypes.c_void_p()
+    uni = ctypes.c_int()
+    check(L.lib().pggc_graph_load(mem.handle, os.fsencode(str(path)), objective, ctypes.byref(uni), ctypes.byref(h)))
+    return weighted_graph(mem, None, None, objective=objective, _handle=h)
+
+
+def graph_from_edges(mem: memory_store, n: int, src, dst, weights=None, symmetric: bool = True,
+                     objective: int = OBJ_MOD) -> weighted_graph:
+    """Builds the CSR of a 0-based edge list on the GPU (construct_from_edgelist,
+    app/io/io_mtx.cpp:95-201): self loops and zero-weight entries dropped,
+    both directions stored, unordered duplicates removed unless ``symmetric``,
+    rows sorted by column.  ``weights`` (int32) only for symmetric lists."""
+    m = int(src.shape[0])
+    if int(dst.shape[0]) != m or (weights is not None and int(weights.shape[0]) != m):
+        raise ValueError("src, dst and weights must have the same length")
+    sp, k1, a1 = _ptr(src, np.int32)
+    dp, k2, a2 = _ptr(dst, np.int32)
+    wp, k3, a3 = (None, None, None) if weights is None else _ptr(weights, np.int32)
+    mk = _one_kind(k1, k2, k3)
+    h = ctypes.c_void_p()
+    check(L.lib().pggc_graph_from_edges(mem.handle, int(n), m, sp, dp, wp, int(bool(symmetric)), objective, mk,
+                                        ctypes.byref(h)))
+    return weighted_graph(mem, None, None, objective=objective, _handle=h)
 
 
 class cluster_data:

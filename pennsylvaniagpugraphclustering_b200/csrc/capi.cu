@@ -3,6 +3,7 @@
 #include <string>
 #include <thread>
 #include "kernels.cuh"
+#include "graph_io.cuh"
 #include "mlp_train.cuh"
 #include "pggc.h"
 
@@ -209,6 +210,24 @@ std::unique_ptr<Graph<W>> make_graph(Context& ctx, int64_t n, int64_t nnz, const
     return g;
 }
 
+// a graph whose CSR already lives in device buffers of `ctx` (graph input):
+// the buffers move in, nothing is copied
+std::unique_ptr<Graph<i32>> adopt_graph(Context& ctx, i64 n, i64 nnz, DBuf<i64>&& rowptr, DBuf<i32>&& col,
+                                        DBuf<i32>&& w, bool uniform, int objective) {
+    auto g = std::make_unique<Graph<i32>>();
+    g->n = n;
+    g->nnz = nnz;
+    g->uniform = uniform;
+    g->rowptr = std::move(rowptr);
+    g->col = std::move(col);
+    if (!uniform) g->w = std::move(w);
+    validate_csr_device(ctx, g->rowptr.p, g->col.p, n, nnz);
+    default_vertex_weights<i32>(ctx, *g, objective);
+    row_sums<i32>(ctx, *g);
+    ctx.sync();
+    return g;
+}
+
 template <class F>
 void dispatch(const pggc_graph* g, F f) {
     if (g->is_float()) f(*g->gf, (double*)nullptr);
@@ -354,6 +373,118 @@ pggc_status pggc_graph_create(pggc_context* ctx, int64_t n, int64_t nnz, const i
             delete g;
             throw;
         }
+        *out = g;
+    });
+}
+
+pggc_status pggc_graph_from_edges(pggc_context* ctx, int64_t n, int64_t m, const int32_t* src, const int32_t* dst,
+                                  const int32_t* weights, int symmetric, int objective, int mem_kind,
+                                  pggc_graph** out) {
+    return guarded([&] {
+        need(ctx && out, "NULL argument");
+        need(n >= 0 && n < 2147483647 && m >= 0, "n must be in [0, 2^31-1) and m >= 0");
+        need(m == 0 || (src && dst), "src or dst is NULL");
+        need(weights == nullptr || symmetric, "weights are only kept for symmetric edge lists");
+        need(objective >= PGGC_OBJ_MOD && objective <= PGGC_OBJ_LCC, "unknown objective");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        c.sync();
+        DBuf<i32> ds, dd, dw;
+        const i32 *ps = src, *pd = dst, *pw = weights;
+        if (mem_kind == PGGC_MEM_HOST && m > 0) {
+            ds = DBuf<i32>(c, m);
+            dd = DBuf<i32>(c, m);
+            PGGC_CUDA(cudaMemcpyAsync(ds.p, src, sizeof(i32) * m, cudaMemcpyHostToDevice, c.stream));
+            PGGC_CUDA(cudaMemcpyAsync(dd.p, dst, sizeof(i32) * m, cudaMemcpyHostToDevice, c.stream));
+            ps = ds.p;
+            pd = dd.p;
+            if (weights) {
+                dw = DBuf<i32>(c, m);
+                PGGC_CUDA(cudaMemcpyAsync(dw.p, weights, sizeof(i32) * m, cudaMemcpyHostToDevice, c.stream));
+                pw = dw.p;
+            }
+        }
+        if (m > 0) {
+            DBuf<int> bad(c, 1);
+            check_edge_ids(c, ps, pd, m, n, bad.p);
+            need(c.read1(bad.p) == 0, "edge endpoint out of range");
+        }
+        DBuf<i64> rp;
+        DBuf<i32> col, w;
+        const i64 nnz = build_csr_from_edges(c, n, m, ps, pd, pw, symmetric != 0, rp, col, w);
+        ds.reset();
+        dd.reset();
+        dw.reset();
+        const bool uniform = pw == nullptr;
+        auto* g = new pggc_graph(ctx);
+        g->kind = uniform ? PGGC_W_UNIFORM : PGGC_W_INT32;
+        try {
+            g->gi = adopt_graph(c, n, nnz, std::move(rp), std::move(col), std::move(w), uniform, objective);
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        *out = g;
+    });
+}
+
+pggc_status pggc_graph_load(pggc_context* ctx, const char* path, int objective, int* edge_uniform_out,
+                            pggc_graph** out) {
+    return guarded([&] {
+        need(ctx && path && out, "NULL argument");
+        need(objective >= PGGC_OBJ_MOD && objective <= PGGC_OBJ_LCC, "unknown objective");
+        Context& c = *ctx->ctx;
+        c.sync();
+        // Mod and CPM read no edge weights (app/objective_helpers.hpp:24-29)
+        bool uniform = objective == PGGC_OBJ_MOD || objective == PGGC_OBJ_CPM;
+        const std::string p(path);
+        const bool mtx = p.size() >= 4 && p.compare(p.size() - 4, 4, ".mtx") == 0;
+        auto* g = new pggc_graph(ctx);
+        try {
+            if (mtx) {
+                EdgeList el;
+                parse_mtx(p, uniform, el);
+                const i64 m = (i64)el.src.size();
+                DBuf<i32> ds(c, std::max<i64>(m, 1)), dd(c, std::max<i64>(m, 1)), dw;
+                if (m > 0) {
+                    PGGC_CUDA(cudaMemcpyAsync(ds.p, el.src.data(), sizeof(i32) * m, cudaMemcpyHostToDevice, c.stream));
+                    PGGC_CUDA(cudaMemcpyAsync(dd.p, el.dst.data(), sizeof(i32) * m, cudaMemcpyHostToDevice, c.stream));
+                }
+                if (el.weighted) {
+                    dw = DBuf<i32>(c, std::max<i64>(m, 1));
+                    if (m > 0)
+                        PGGC_CUDA(cudaMemcpyAsync(dw.p, el.w.data(), sizeof(i32) * m, cudaMemcpyHostToDevice, c.stream));
+                }
+                DBuf<i64> rp;
+                DBuf<i32> col, w;
+                const i64 nnz =
+                    build_csr_from_edges(c, el.n, m, ds.p, dd.p, el.weighted ? dw.p : nullptr, el.symmetric, rp, col, w);
+                c.sync();  // the host edge list is released next
+                g->kind = el.weighted ? PGGC_W_INT32 : PGGC_W_UNIFORM;
+                g->gi = adopt_graph(c, el.n, nnz, std::move(rp), std::move(col), std::move(w), !el.weighted, objective);
+            } else {
+                CsrHost h;
+                parse_metis(p, uniform, h);
+                const i64 nnz = (i64)h.col.size();
+                DBuf<i64> rp(c, h.n + 1);
+                DBuf<i32> col(c, std::max<i64>(nnz, 1)), w;
+                PGGC_CUDA(cudaMemcpyAsync(rp.p, h.rowptr.data(), sizeof(i64) * (h.n + 1), cudaMemcpyHostToDevice,
+                                          c.stream));
+                if (nnz > 0)
+                    PGGC_CUDA(cudaMemcpyAsync(col.p, h.col.data(), sizeof(i32) * nnz, cudaMemcpyHostToDevice, c.stream));
+                if (h.weighted) {
+                    w = DBuf<i32>(c, std::max<i64>(nnz, 1));
+                    if (nnz > 0)
+                        PGGC_CUDA(cudaMemcpyAsync(w.p, h.w.data(), sizeof(i32) * nnz, cudaMemcpyHostToDevice, c.stream));
+                }
+                g->kind = h.weighted ? PGGC_W_INT32 : PGGC_W_UNIFORM;
+                g->gi = adopt_graph(c, h.n, nnz, std::move(rp), std::move(col), std::move(w), !h.weighted, objective);
+            }
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        if (edge_uniform_out) *edge_uniform_out = g->kind == PGGC_W_UNIFORM ? 1 : 0;
         *out = g;
     });
 }
