@@ -15,7 +15,12 @@
  *   - Weight kinds: PGGC_W_UNIFORM (unit weights, `weights` ignored),
  *     PGGC_W_INT32 (int32 weights), PGGC_W_FLOAT32 (float32 weights).
  *     Vertex weights / cluster volumes ("V" arrays) are int64 for the first two
- *     and float64 for PGGC_W_FLOAT32.
+ *     and float64 for PGGC_W_FLOAT32.  Float64 volumes are summed with
+ *     order-free atomics, so results are bit-reproducible when every vertex
+ *     weight is a multiple of one power of two q and the total weight stays
+ *     below 2^53 q (the default weighted degrees of FP32 weights in [0.5, 1.5)
+ *     meet it for nnz < 2^29); other float64 vertex weights can differ
+ *     between runs in the last bits.
  *   - Graphs are symmetric CSR: int64 row offsets (n+1), int32 columns (nnz),
  *     no self-loops, no duplicate edges.
  *   - Calls on one context are serialised on the context's CUDA stream and
@@ -113,6 +118,9 @@ pggc_status pggc_graph_load(pggc_context* ctx, const char* path, int objective, 
 pggc_status pggc_graph_from_edges(pggc_context* ctx, int64_t n, int64_t m, const int32_t* src, const int32_t* dst,
                                   const int32_t* weights, int symmetric, int objective, int mem_kind,
                                   pggc_graph** out);
+/* replaces the vertex weights (n values: int64, or double for FP32-weighted
+ * graphs), as get_vtx_weights does with -vw_file (app/io/vertex_weighting.cpp:27-30) */
+pggc_status pggc_graph_set_vertex_weights(pggc_context* ctx, pggc_graph* g, const void* vtx_w, int mem_kind);
 pggc_status pggc_graph_destroy(pggc_graph* g);
 pggc_status pggc_graph_dims(const pggc_graph* g, int64_t* n, int64_t* nnz, int* weight_kind);
 /* copies out any non-NULL array (weights only for non-uniform graphs) */

@@ -81,6 +81,11 @@ def lib():
         L.orc_signature.argtypes = [vp, vp, vp]
         L.orc_meme_cluster.argtypes = [vp, ci, dbl, ci, i64, u64, vp, ctypes.POINTER(MemeStats)]
         L.orc_meme_cluster.restype = ci
+        L.orc_run_clustering.restype = ci
+        L.orc_leiden_part.restype = ci
+        L.orc_louvain_part.restype = ci
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_last_error.argtypes = []
         _LIB = L
     return _LIB
 
@@ -185,6 +190,11 @@ def select(g: Graph, cd: ClusterData, part, pvals, dest, filter_ratio, initial, 
     return dest, gain, int(k)
 
 
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+
+
 def local_move(g: Graph, cd: ClusterData, part, is_initial, enable_sa=True, strict=False, constrained=False,
                constraint=None, sweep_limit=-1):
     part = np.array(part, np.int32, copy=True)
@@ -206,7 +216,7 @@ def coarsen_leidenR(g: Graph, cd: ClusterData, constraint, seed_pick, seed_order
 def run_clustering(g: Graph, cd: ClusterData, method=METHOD_LEIDEN_PLUS, ex_iters=0, seed=1):
     out = np.empty(g.n, np.int32)
     st = Stats()
-    lib().orc_run_clustering(g.h, cd.h, method, ex_iters, seed, _p(out), ctypes.byref(st))
+    _check(lib().orc_run_clustering(g.h, cd.h, method, ex_iters, seed, _p(out), ctypes.byref(st)))
     return out, st
 
 
@@ -214,7 +224,7 @@ def leiden_part(g: Graph, cd: ClusterData, plus=True, improve=False, input_part=
     out = np.empty(g.n, np.int32)
     st = Stats()
     inp = None if input_part is None else np.ascontiguousarray(input_part, np.int32)
-    lib().orc_leiden_part(g.h, cd.h, int(plus), int(improve), _p(inp), seed, _p(out), ctypes.byref(st))
+    _check(lib().orc_leiden_part(g.h, cd.h, int(plus), int(improve), _p(inp), seed, _p(out), ctypes.byref(st)))
     return out, st
 
 
@@ -222,7 +232,7 @@ def louvain_part(g: Graph, cd: ClusterData, constrained=False, constraint=None):
     out = np.empty(g.n, np.int32)
     st = Stats()
     con = None if constraint is None else np.ascontiguousarray(constraint, np.int32)
-    lib().orc_louvain_part(g.h, cd.h, int(constrained), _p(con), _p(out), ctypes.byref(st))
+    _check(lib().orc_louvain_part(g.h, cd.h, int(constrained), _p(con), _p(out), ctypes.byref(st)))
     return out, st
 
 
@@ -276,5 +286,5 @@ def signature(g: Graph, labels):
 def meme_cluster(g: Graph, objective, lambda_mult=1.0, pop_size=8, offspring=16, seed=1):
     out = np.empty(g.n, np.int32)
     st = MemeStats()
-    lib().orc_meme_cluster(g.h, objective, float(lambda_mult), pop_size, offspring, seed, _p(out), ctypes.byref(st))
+    _check(lib().orc_meme_cluster(g.h, objective, float(lambda_mult), pop_size, offspring, seed, _p(out), ctypes.byref(st)))
     return out, st

@@ -45,6 +45,8 @@
 #include <memory>
 #include <numeric>
 #include <stdexcept>
+#include <deque>
+#include <string>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1083,11 +1085,10 @@ struct Engine {
     // ---- leiden_part<plus,improve>, src/clustering_methods.cpp:47-137
     std::vector<i32> leiden_part(const G& top, CD& rfd, bool plus, bool improve, const i32* input, u64 seed,
                                  i64* level_count, i64* total_nnz) {
-        std::vector<G> coarse;   // owned coarse graphs
+        std::deque<G> coarse;  // owned coarse graphs; a deque keeps references stable
         std::vector<const G*> levels;
         std::vector<std::vector<i32>> parts;
         levels.push_back(&top);
-        coarse.reserve(256);
         std::vector<i32> part(top.n);
         if (!improve)
             for (i64 x = 0; x < top.n; x++) part[x] = (i32)x;
@@ -1152,8 +1153,7 @@ struct Engine {
             rfd.label_count = top.n;
             rfd.update_objective();
         }
-        std::vector<G> coarse;
-        coarse.reserve(256);
+        std::deque<G> coarse;  // owned coarse graphs; a deque keeps references stable
         std::vector<const G*> levels;
         std::vector<std::vector<i32>> parts;
         levels.push_back(&top);
@@ -1306,7 +1306,22 @@ static void fill_graph(Graph<W>& g, int kind, int64_t n, int64_t nnz, const int6
     }
 }
 
+// the level loops throw when a hierarchy passes 4096 levels; the C entry points
+// turn exceptions into -1 and keep the message for orc_last_error
+static thread_local std::string orc_error;
+template <class F>
+static int orc_guard(F f) {
+    try {
+        return f();
+    } catch (const std::exception& e) {
+        orc_error = e.what();
+        return -1;
+    }
+}
+
 extern "C" {
+
+const char* orc_last_error() { return orc_error.c_str(); }
 
 void* orc_graph_new(int64_t n, int64_t nnz, const int64_t* rowptr, const int32_t* col, const void* w, int wkind,
                     const void* vtx_w, int objective) {
@@ -1508,111 +1523,117 @@ int64_t orc_coarsen_leidenR(void* gh, void* cdh, const int32_t* constraint, uint
 // method: 0 louvain (plouvain), 1 leiden (pleiden), 2 leiden+ (pleiden+).
 // ex_iters as in app/cluster_main.cpp:101-114 (negative: until the objective stops rising).
 int orc_run_clustering(void* gh, void* cdh, int method, int ex_iters, uint64_t seed, int32_t* labels_out, OrcStats* st) {
-    auto* g = (OrcGraph*)gh;
-    auto* cd = (OrcCD*)cdh;
-    auto run = [&](auto& eng, auto& gg, auto& c) {
-        i64 lv = 0, tn = 0;
-        std::vector<i32> part;
-        u64 pass = 0;
-        auto one = [&](bool improve, const std::vector<i32>* input) {
-            if (method == 0) {
-                std::vector<i32> con;
-                if (improve) con = *input;
-                return eng.louvain_part(gg, c, improve, con, &lv, &tn);
+    return orc_guard([&]() -> int {
+        auto* g = (OrcGraph*)gh;
+        auto* cd = (OrcCD*)cdh;
+        auto run = [&](auto& eng, auto& gg, auto& c) {
+            i64 lv = 0, tn = 0;
+            std::vector<i32> part;
+            u64 pass = 0;
+            auto one = [&](bool improve, const std::vector<i32>* input) {
+                if (method == 0) {
+                    std::vector<i32> con;
+                    if (improve) con = *input;
+                    return eng.louvain_part(gg, c, improve, con, &lv, &tn);
+                }
+                u64 s = seed + 0x9E3779B97F4A7C15ull * pass;
+                pass++;
+                return eng.leiden_part(gg, c, method == 2, improve, improve ? input->data() : nullptr, s, &lv, &tn);
+            };
+            part = one(false, nullptr);
+            double last = -std::numeric_limits<double>::infinity();
+            int counter = 0;
+            while (true) {
+                bool terminate = true;
+                if (ex_iters < 0) {
+                    if (c.get_objective() > last) terminate = false;
+                    last = c.get_objective();
+                } else {
+                    if (counter++ < ex_iters) terminate = false;
+                }
+                if (terminate) break;
+                std::vector<i32> con = part;
+                part = one(true, &con);
             }
-            u64 s = seed + 0x9E3779B97F4A7C15ull * pass;
-            pass++;
-            return eng.leiden_part(gg, c, method == 2, improve, improve ? input->data() : nullptr, s, &lv, &tn);
+            std::copy(part.begin(), part.end(), labels_out);
+            if (st) {
+                st->levels = lv;
+                st->total_nnz = tn;
+                st->sweeps = eng.total_sweeps;
+                st->moves = eng.total_moves;
+                st->objective = c.get_objective();
+                st->raw_obj = c.obj;
+                st->label_count = c.label_count;
+            }
+            return 0;
         };
-        part = one(false, nullptr);
-        double last = -std::numeric_limits<double>::infinity();
-        int counter = 0;
-        while (true) {
-            bool terminate = true;
-            if (ex_iters < 0) {
-                if (c.get_objective() > last) terminate = false;
-                last = c.get_objective();
-            } else {
-                if (counter++ < ex_iters) terminate = false;
-            }
-            if (terminate) break;
-            std::vector<i32> con = part;
-            part = one(true, &con);
+        if (g->kind == 2) {
+            Engine<float> e;
+            return run(e, g->gf, cd->cf);
         }
-        std::copy(part.begin(), part.end(), labels_out);
-        if (st) {
-            st->levels = lv;
-            st->total_nnz = tn;
-            st->sweeps = eng.total_sweeps;
-            st->moves = eng.total_moves;
-            st->objective = c.get_objective();
-            st->raw_obj = c.obj;
-            st->label_count = c.label_count;
-        }
-        return 0;
-    };
-    if (g->kind == 2) {
-        Engine<float> e;
-        return run(e, g->gf, cd->cf);
-    }
-    Engine<i32> e;
-    return run(e, g->gi, cd->ci);
+        Engine<i32> e;
+        return run(e, g->gi, cd->ci);
+    });
 }
 
 // leiden_part / louvain_part, one call (no ex_iters loop).
 int orc_leiden_part(void* gh, void* cdh, int plus, int improve, const int32_t* input, uint64_t seed, int32_t* labels_out,
                     OrcStats* st) {
-    auto* g = (OrcGraph*)gh;
-    auto* cd = (OrcCD*)cdh;
-    auto run = [&](auto& eng, auto& gg, auto& c) {
-        i64 lv = 0, tn = 0;
-        auto part = eng.leiden_part(gg, c, plus != 0, improve != 0, input, seed, &lv, &tn);
-        std::copy(part.begin(), part.end(), labels_out);
-        if (st) {
-            st->levels = lv;
-            st->total_nnz = tn;
-            st->sweeps = eng.total_sweeps;
-            st->moves = eng.total_moves;
-            st->objective = c.get_objective();
-            st->raw_obj = c.obj;
-            st->label_count = c.label_count;
+    return orc_guard([&]() -> int {
+        auto* g = (OrcGraph*)gh;
+        auto* cd = (OrcCD*)cdh;
+        auto run = [&](auto& eng, auto& gg, auto& c) {
+            i64 lv = 0, tn = 0;
+            auto part = eng.leiden_part(gg, c, plus != 0, improve != 0, input, seed, &lv, &tn);
+            std::copy(part.begin(), part.end(), labels_out);
+            if (st) {
+                st->levels = lv;
+                st->total_nnz = tn;
+                st->sweeps = eng.total_sweeps;
+                st->moves = eng.total_moves;
+                st->objective = c.get_objective();
+                st->raw_obj = c.obj;
+                st->label_count = c.label_count;
+            }
+            return 0;
+        };
+        if (g->kind == 2) {
+            Engine<float> e;
+            return run(e, g->gf, cd->cf);
         }
-        return 0;
-    };
-    if (g->kind == 2) {
-        Engine<float> e;
-        return run(e, g->gf, cd->cf);
-    }
-    Engine<i32> e;
-    return run(e, g->gi, cd->ci);
+        Engine<i32> e;
+        return run(e, g->gi, cd->ci);
+    });
 }
 
 int orc_louvain_part(void* gh, void* cdh, int constrained, const int32_t* constraint, int32_t* labels_out, OrcStats* st) {
-    auto* g = (OrcGraph*)gh;
-    auto* cd = (OrcCD*)cdh;
-    auto run = [&](auto& eng, auto& gg, auto& c) {
-        i64 lv = 0, tn = 0;
-        std::vector<i32> con;
-        if (constrained) con.assign(constraint, constraint + gg.n);
-        auto part = eng.louvain_part(gg, c, constrained != 0, con, &lv, &tn);
-        std::copy(part.begin(), part.end(), labels_out);
-        if (st) {
-            st->levels = lv;
-            st->total_nnz = tn;
-            st->sweeps = eng.total_sweeps;
-            st->moves = eng.total_moves;
-            st->objective = c.get_objective();
-            st->raw_obj = c.obj;
-            st->label_count = c.label_count;
+    return orc_guard([&]() -> int {
+        auto* g = (OrcGraph*)gh;
+        auto* cd = (OrcCD*)cdh;
+        auto run = [&](auto& eng, auto& gg, auto& c) {
+            i64 lv = 0, tn = 0;
+            std::vector<i32> con;
+            if (constrained) con.assign(constraint, constraint + gg.n);
+            auto part = eng.louvain_part(gg, c, constrained != 0, con, &lv, &tn);
+            std::copy(part.begin(), part.end(), labels_out);
+            if (st) {
+                st->levels = lv;
+                st->total_nnz = tn;
+                st->sweeps = eng.total_sweeps;
+                st->moves = eng.total_moves;
+                st->objective = c.get_objective();
+                st->raw_obj = c.obj;
+                st->label_count = c.label_count;
+            }
+            return 0;
+        };
+        if (g->kind == 2) {
+            Engine<float> e;
+            return run(e, g->gf, cd->cf);
         }
-        return 0;
-    };
-    if (g->kind == 2) {
-        Engine<float> e;
-        return run(e, g->gf, cd->cf);
-    }
-    Engine<i32> e;
-    return run(e, g->gi, cd->ci);
+        Engine<i32> e;
+        return run(e, g->gi, cd->ci);
+    });
 }
 
 // ---- memetic driver, app/memetic_clustering.cpp:27-219 ---------------------
@@ -1660,96 +1681,98 @@ static inline int64_t orc_uniform_below(SplitMix64& r, int64_t m) {
 // the random stream matches the GPU driver's call for call
 int orc_meme_cluster(void* gh, int objective, double mult, int pop_size, int64_t offspring, uint64_t seed,
                      int32_t* labels_out, OrcMemeStats* st) {
-    auto* g = (OrcGraph*)gh;
-    auto run = [&](auto& eng, auto& gg) {
-        using W = typename std::remove_reference_t<decltype(gg)>::Weight;
-        const int64_t n = gg.n;
-        const int64_t words = (std::max<int64_t>(gg.nnz, 1) + 31) / 32;
-        struct Member {
-            std::vector<i32> clusters;
-            std::vector<uint32_t> sign;
-            double obj = 0;
-            int64_t labels = 0;
-        };
-        std::vector<Member> pop((size_t)pop_size);
-        SplitMix64 rng(seed);
-        double best_initial = -std::numeric_limits<double>::infinity();
-        auto signature = [&](const std::vector<i32>& c, std::vector<uint32_t>& s) {
-            s.assign((size_t)words, 0u);
-            for (int64_t i = 0; i < n; i++)
-                for (int64_t j = gg.rowptr[i]; j < gg.rowptr[i + 1]; j++)
-                    if (c[i] != c[gg.col[j]]) s[j / 32] |= 1u << (j % 32);
-        };
-        i64 lv = 0, tn = 0;
-        for (int p = 0; p < pop_size; p++) {
-            auto cd = make_objective<W>(gg, objective, mult);
-            pop[p].clusters = eng.leiden_part(gg, cd, true, false, nullptr, rng.next(), &lv, &tn);
-            pop[p].obj = cd.get_objective();
-            pop[p].labels = cd.label_count;
-            signature(pop[p].clusters, pop[p].sign);
-            best_initial = std::max(best_initial, pop[p].obj);
-        }
-        auto pick = [&]() {
-            const int64_t a = orc_uniform_below(rng, pop_size);
-            const int64_t b = (a + orc_uniform_below(rng, pop_size - 1)) % pop_size;
-            return pop[a].obj > pop[b].obj ? a : b;
-        };
-        int64_t made = 0, replaced = 0;
-        std::vector<i32> constraint((size_t)n);
-        std::vector<uint32_t> csign;
-        while (made < offspring) {
-            const int64_t p1 = pick();
-            int64_t p2 = p1;
-            while (p2 == p1) p2 = pick();
-            orc_intersect(pop[p1].clusters.data(), pop[p2].clusters.data(), n, constraint.data());
-            auto cd = make_objective<W>(gg, objective, mult);
-            std::vector<i32> child = eng.louvain_part(gg, cd, true, constraint, &lv, &tn);
-            for (int x = 0; x < 5; x++) {
-                std::vector<i32> in = child;
-                child = eng.leiden_part(gg, cd, true, true, in.data(), rng.next(), &lv, &tn);
-            }
-            made++;
-            const double obj = cd.get_objective();
-            signature(child, csign);
-            int64_t am = -1;
-            int64_t min_diff = std::numeric_limits<int64_t>::max();
+    return orc_guard([&]() -> int {
+        auto* g = (OrcGraph*)gh;
+        auto run = [&](auto& eng, auto& gg) {
+            using W = typename std::remove_reference_t<decltype(gg)>::Weight;
+            const int64_t n = gg.n;
+            const int64_t words = (std::max<int64_t>(gg.nnz, 1) + 31) / 32;
+            struct Member {
+                std::vector<i32> clusters;
+                std::vector<uint32_t> sign;
+                double obj = 0;
+                int64_t labels = 0;
+            };
+            std::vector<Member> pop((size_t)pop_size);
+            SplitMix64 rng(seed);
+            double best_initial = -std::numeric_limits<double>::infinity();
+            auto signature = [&](const std::vector<i32>& c, std::vector<uint32_t>& s) {
+                s.assign((size_t)words, 0u);
+                for (int64_t i = 0; i < n; i++)
+                    for (int64_t j = gg.rowptr[i]; j < gg.rowptr[i + 1]; j++)
+                        if (c[i] != c[gg.col[j]]) s[j / 32] |= 1u << (j % 32);
+            };
+            i64 lv = 0, tn = 0;
             for (int p = 0; p < pop_size; p++) {
-                if (pop[p].obj < obj) {
-                    int64_t d = 0;
-                    for (int64_t w = 0; w < words; w++) d += __builtin_popcount(csign[w] ^ pop[p].sign[w]);
-                    if (d < min_diff) {
-                        min_diff = d;
-                        am = p;
+                auto cd = make_objective<W>(gg, objective, mult);
+                pop[p].clusters = eng.leiden_part(gg, cd, true, false, nullptr, rng.next(), &lv, &tn);
+                pop[p].obj = cd.get_objective();
+                pop[p].labels = cd.label_count;
+                signature(pop[p].clusters, pop[p].sign);
+                best_initial = std::max(best_initial, pop[p].obj);
+            }
+            auto pick = [&]() {
+                const int64_t a = orc_uniform_below(rng, pop_size);
+                const int64_t b = (a + orc_uniform_below(rng, pop_size - 1)) % pop_size;
+                return pop[a].obj > pop[b].obj ? a : b;
+            };
+            int64_t made = 0, replaced = 0;
+            std::vector<i32> constraint((size_t)n);
+            std::vector<uint32_t> csign;
+            while (made < offspring) {
+                const int64_t p1 = pick();
+                int64_t p2 = p1;
+                while (p2 == p1) p2 = pick();
+                orc_intersect(pop[p1].clusters.data(), pop[p2].clusters.data(), n, constraint.data());
+                auto cd = make_objective<W>(gg, objective, mult);
+                std::vector<i32> child = eng.louvain_part(gg, cd, true, constraint, &lv, &tn);
+                for (int x = 0; x < 5; x++) {
+                    std::vector<i32> in = child;
+                    child = eng.leiden_part(gg, cd, true, true, in.data(), rng.next(), &lv, &tn);
+                }
+                made++;
+                const double obj = cd.get_objective();
+                signature(child, csign);
+                int64_t am = -1;
+                int64_t min_diff = std::numeric_limits<int64_t>::max();
+                for (int p = 0; p < pop_size; p++) {
+                    if (pop[p].obj < obj) {
+                        int64_t d = 0;
+                        for (int64_t w = 0; w < words; w++) d += __builtin_popcount(csign[w] ^ pop[p].sign[w]);
+                        if (d < min_diff) {
+                            min_diff = d;
+                            am = p;
+                        }
                     }
                 }
+                if (am >= 0) {
+                    pop[am].clusters = child;
+                    pop[am].sign = csign;
+                    pop[am].obj = obj;
+                    pop[am].labels = cd.label_count;
+                    replaced++;
+                }
             }
-            if (am >= 0) {
-                pop[am].clusters = child;
-                pop[am].sign = csign;
-                pop[am].obj = obj;
-                pop[am].labels = cd.label_count;
-                replaced++;
+            int am = 0;
+            for (int p = 1; p < pop_size; p++)
+                if (pop[p].obj > pop[am].obj) am = p;
+            std::copy(pop[am].clusters.begin(), pop[am].clusters.end(), labels_out);
+            if (st) {
+                st->objective = pop[am].obj;
+                st->label_count = pop[am].labels;
+                st->offspring = made;
+                st->replaced = replaced;
+                st->best_initial = best_initial;
             }
+            return 0;
+        };
+        if (g->kind == 2) {
+            Engine<float> e;
+            return run(e, g->gf);
         }
-        int am = 0;
-        for (int p = 1; p < pop_size; p++)
-            if (pop[p].obj > pop[am].obj) am = p;
-        std::copy(pop[am].clusters.begin(), pop[am].clusters.end(), labels_out);
-        if (st) {
-            st->objective = pop[am].obj;
-            st->label_count = pop[am].labels;
-            st->offspring = made;
-            st->replaced = replaced;
-            st->best_initial = best_initial;
-        }
-        return 0;
-    };
-    if (g->kind == 2) {
-        Engine<float> e;
-        return run(e, g->gf);
-    }
-    Engine<i32> e;
-    return run(e, g->gi);
+        Engine<i32> e;
+        return run(e, g->gi);
+    });
 }
 
 double orc_verify_objective(void* gh, const int32_t* labels, int objective, double mult, double* raw_obj) {

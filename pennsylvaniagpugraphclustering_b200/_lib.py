@@ -75,6 +75,7 @@ _SIGS = {
     "pggc_context_stream": (_ci, [_vp, _PP]),
     "pggc_graph_create": (_ci, [_vp, _i64, _i64, _vp, _vp, _vp, _ci, _vp, _ci, _ci, _PP]),
     "pggc_graph_destroy": (_ci, [_vp]),
+    "pggc_graph_set_vertex_weights": (_ci, [_vp, _vp, _vp, _ci]),
     "pggc_graph_load": (_ci, [_vp, ctypes.c_char_p, _ci, ctypes.POINTER(_ci), _PP]),
     "pggc_graph_from_edges": (_ci, [_vp, _i64, _i64, _vp, _vp, _vp, _ci, _ci, _ci, _PP]),
     "pggc_graph_dims": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_ci)]),

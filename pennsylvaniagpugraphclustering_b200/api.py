@@ -169,6 +169,13 @@ class weighted_graph:
                                       None if w is None else w.ctypes.data, vw.ctypes.data, MEM_HOST))
         return rowptr, col, w, vw
 
+    def set_vertex_weights(self, vtx_w):
+        """Replaces the vertex weights (``n`` values; int64, or float64 for FP32-weighted graphs)."""
+        if int(vtx_w.shape[0]) != self.n:
+            raise ValueError(f"vtx_w has {int(vtx_w.shape[0])} values, the graph {self.n} vertices")
+        vp, k, a = _ptr(vtx_w, self.vdtype)
+        check(L.lib().pggc_graph_set_vertex_weights(self.mem.handle, self._h, vp, k))
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             L.lib().pggc_graph_destroy(self._h)
@@ -181,19 +188,49 @@ class weighted_graph:
             pass
 
 
-def load_graph(mem: memory_store, path, objective: int = OBJ_MOD) -> weighted_graph:
+def load_graph(mem: memory_store, path, objective: int = OBJ_MOD, vtx_w=None) -> weighted_graph:
     """Reads a Matrix Market (``.mtx``) or METIS file into a device graph
     (load_graph, app/io/io_mtx.cpp:336-345; load_mtx_graph :204-333;
     load_metis_graph, app/io/io_metis.cpp:64-181).
 
     Mod and CPM ignore file weights; ``wg.edge_uniform`` is the reference's
-    ``uniform_ew`` after loading.  Malformed files raise ``PggcError``.
+    ``uniform_ew`` after loading.  ``vtx_w`` (n values, e.g. from
+    :func:`load_view`) replaces the objective's default vertex weights, as
+    ``-vw_file`` does (app/io/vertex_weighting.cpp:27-30).  Malformed files
+    raise ``PggcError``.
     """
     h = ctypes.c_void_p()
     uni = ctypes.c_int()
     check(L.lib().pggc_graph_load(mem.handle, os.fsencode(str(path)), objective, ctypes.byref(uni), ctypes.byref(h)))
-    return weighted_graph(mem, None, None, objective=objective, _handle=h)
+    wg = weighted_graph(mem, None, None, objective=objective, _handle=h)
+    if vtx_w is not None:
+        wg.set_vertex_weights(vtx_w)
+    return wg
 
+
+def load_view(n: int, path, dtype=np.int64) -> np.ndarray:
+    """``load_view<view_t>(n, fname)`` (app/io/header/io_views.hpp:26-41): the
+    first ``n`` whitespace-separated values of a text file (vertex weights for
+    ``-vw_file``, a clustering for verify_objective).  A file that cannot be
+    opened raises ``InvalidArgument`` (the reference prints FATAL ERROR and
+    returns zeros); values the file does not hold stay 0, as in the reference."""
+    try:
+        with open(path, "rb") as fh:
+            tokens = fh.read().split()
+    except OSError as e:
+        raise L.InvalidArgument(L.PGGC_ERR_INVALID, f"could not open {path}: {e}") from None
+    out = np.zeros(int(n), dtype)
+    k = min(int(n), len(tokens))
+    if k:
+        out[:k] = np.array(tokens[:k]).astype(dtype)
+    return out
+
+
+def write_part(labels, path) -> None:
+    """``write_part`` (app/io/header/io_views.hpp:11-24): one label per line."""
+    a = np.asarray(labels.cpu() if hasattr(labels, "cpu") else labels).ravel()
+    with open(path, "w") as fh:
+        fh.write("".join(f"{int(x)}\n" for x in a))
 
 def graph_from_edges(mem: memory_store, n: int, src, dst, weights=None, symmetric: bool = True,
                      objective: int = OBJ_MOD) -> weighted_graph:

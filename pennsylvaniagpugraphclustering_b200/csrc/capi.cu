@@ -489,6 +489,24 @@ pggc_status pggc_graph_load(pggc_context* ctx, const char* path, int objective, 
     });
 }
 
+pggc_status pggc_graph_set_vertex_weights(pggc_context* ctx, pggc_graph* g, const void* vtx_w, int mem_kind) {
+    return guarded([&] {
+        need(ctx && g && vtx_w, "NULL argument");
+        check_mem_kind(mem_kind);
+        Context& c = *ctx->ctx;
+        auto kindc = mem_kind == PGGC_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        c.sync();
+        if (g->is_float()) {
+            if (g->gf->n > 0)
+                PGGC_CUDA(cudaMemcpyAsync(g->gf->vtx_w.p, vtx_w, sizeof(double) * g->gf->n, kindc, c.stream));
+        } else {
+            if (g->gi->n > 0)
+                PGGC_CUDA(cudaMemcpyAsync(g->gi->vtx_w.p, vtx_w, sizeof(i64) * g->gi->n, kindc, c.stream));
+        }
+        c.sync();
+    });
+}
+
 pggc_status pggc_graph_destroy(pggc_graph* g) {
     return guarded([&] { delete g; });
 }

@@ -94,3 +94,24 @@ def small_dcsbm(seed=1, n=20000):
 
 def small_rmat(seed=1, scale=12):
     return gg.rmat(scale, 16, 0.57, 0.19, 0.19, seed)
+
+
+def int_weighted(hg, scale=4.0):
+    """The same graph with int32 edge weights round(scale * w) (symmetric
+    because w is): the reference's own weight type."""
+    w = np.maximum(np.rint(hg.w.astype(np.float64) * scale), 1).astype(np.int32)
+    return HostGraph(hg.rowptr, hg.col, w, name=hg.name + "+int")
+
+
+def with_vertex_weights(hg, seed):
+    """The same graph carrying custom vertex weights ``vw`` (int64 for uniform or
+    int32-weighted graphs, float64 for FP32-weighted ones)."""
+    rng = np.random.default_rng(seed)
+    g = HostGraph(hg.rowptr, hg.col, hg.w, name=hg.name + "+vw")
+    if hg.w is not None and hg.w.dtype == np.float32:
+        # FP32 values: their FP64 sums are exact in any order, the condition
+        # for bit-reproducible cluster volumes
+        g.vw = rng.uniform(0.5, 3.0, hg.n).astype(np.float32).astype(np.float64)
+    else:
+        g.vw = rng.integers(1, 21, hg.n).astype(np.int64)
+    return g

@@ -184,3 +184,28 @@ def test_loaded_graph_clusters_like_the_oracle_csr(mem, tmp_path):
         labels, st = pg.run_clustering(mem, g, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=4)
         out.append((labels, st["objective"]))
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+def test_vertex_weight_file_feeds_the_objective(mem, tmp_path):
+    """-vw_file: load_view + load_graph(vtx_w=...) equals the oracle given the
+    same weights (CPM, where vertex weights are the cluster sizes)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(13)
+    p = tmp_path / "g.mtx"
+    p.write_bytes(_mtx_text(rng, 2000, 12000, "pattern", True, comments=False))
+    vwf = tmp_path / "vw.txt"
+    vw = rng.integers(1, 5, 2000).astype(np.int64)
+    pg.write_part(vw, vwf)
+    vw_in = pg.load_view(2000, vwf)
+    assert np.array_equal(vw_in, vw)
+    wg = pg.load_graph(mem, str(p), pg.OBJ_CPM, vtx_w=vw_in)
+    rp, c, _, vg = wg.to_host()
+    assert np.array_equal(vg, vw)
+    og = O.Graph(rp, c, None, vtx_w=vw, objective=pg.OBJ_CPM)
+    cd_o = O.ClusterData(og, pg.OBJ_CPM, 1.0)
+    cd_g = pg.get_objective(mem, wg, pg.OBJ_CPM, 1.0)
+    lo, so = O.run_clustering(og, cd_o, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=2)
+    lg, sg = pg.run_clustering(mem, wg, cd_g, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=2)
+    assert np.array_equal(lo, lg) and so.objective == sg["objective"]
+    with pytest.raises(ValueError):
+        wg.set_vertex_weights(vw[:10])

@@ -19,8 +19,11 @@ pytestmark = pytest.mark.gpu
 def _pair(mem, hg, objective):
     uniform = objective in (pg.OBJ_MOD, pg.OBJ_CPM) or hg.w is None
     w = None if uniform else hg.w
-    og = O.Graph(hg.rowptr, hg.col, w, objective=objective)
-    wg = pg.weighted_graph(mem, hg.rowptr, hg.col, w, objective=objective)
+    vw = getattr(hg, "vw", None)
+    if vw is not None and (w is None or w.dtype != np.float32):
+        vw = vw.astype(np.int64) if vw.dtype != np.int64 else vw
+    og = O.Graph(hg.rowptr, hg.col, w, vtx_w=vw, objective=objective)
+    wg = pg.weighted_graph(mem, hg.rowptr, hg.col, w, objective=objective, vtx_w=vw)
     return og, wg
 
 
@@ -36,6 +39,20 @@ CASES = [
     ("dcsbm_mod", G.small_dcsbm, pg.OBJ_MOD),
     ("hub_wmod", G.hub_graph, pg.OBJ_WMOD),
     ("hub_mod", G.hub_graph, pg.OBJ_MOD),
+    # the other objectives (interface/cluster_data.hpp:109-181)
+    ("sbm_cpm", G.small_sbm, pg.OBJ_CPM),
+    ("hub_cpm", G.hub_graph, pg.OBJ_CPM),
+    ("dcsbm_nlcc", G.small_dcsbm, pg.OBJ_NLCC),
+    ("dcsbm_lcc", G.small_dcsbm, pg.OBJ_LCC),
+    ("hub_lcc", G.hub_graph, pg.OBJ_LCC),
+    # int32 edge weights, the reference's weight type
+    ("dcsbm_int_wmod", lambda: G.int_weighted(G.small_dcsbm()), pg.OBJ_WMOD),
+    ("dcsbm_int_nlcc", lambda: G.int_weighted(G.small_dcsbm()), pg.OBJ_NLCC),
+    ("hub_int_nlcc", lambda: G.int_weighted(G.hub_graph()), pg.OBJ_NLCC),
+    # custom vertex weights (app/io/vertex_weighting.cpp:27-42 replaced by the caller's)
+    ("sbm_mod_vw", lambda: G.with_vertex_weights(G.small_sbm(), 1), pg.OBJ_MOD),
+    ("dcsbm_wmod_vw", lambda: G.with_vertex_weights(G.small_dcsbm(), 2), pg.OBJ_WMOD),
+    ("rmat_cpm_vw", lambda: G.with_vertex_weights(G.small_rmat(), 3), pg.OBJ_CPM),
 ]
 IDS = [c[0] for c in CASES]
 
@@ -295,3 +312,18 @@ def test_select_pass_vertex_wider_than_shared_table(mem, weighted):
         assert ko == kg
         assert np.array_equal(do, dg)
         assert np.array_equal(go.view(np.int32), gg_.view(np.int32))
+
+
+def test_int_weighted_lcc_louvain(mem):
+    """LCC on int32 weights 2..6 at lambda 1: pLouvain parity.  (pLeiden on this
+    graph reaches a level where the refinement contracts nothing while the
+    local move still merges; the reference's level loop has no bound there, and
+    both sides stop with an error after 4096 levels.)"""
+    hg = G.int_weighted(G.small_dcsbm(n=5000))
+    og, wg = _pair(mem, hg, pg.OBJ_LCC)
+    cd_o = O.ClusterData(og, pg.OBJ_LCC, 1.0)
+    cd_g = pg.get_objective(mem, wg, pg.OBJ_LCC, 1.0)
+    lo, so = O.run_clustering(og, cd_o, method=pg.METHOD_LOUVAIN, ex_iters=0, seed=7)
+    lg, sg = pg.run_clustering(mem, wg, cd_g, method=pg.METHOD_LOUVAIN, ex_iters=0, seed=7)
+    assert np.array_equal(lo, lg)
+    assert so.objective == sg["objective"] and so.label_count == sg["label_count"]
