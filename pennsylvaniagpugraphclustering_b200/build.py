@@ -4,7 +4,9 @@ Outputs go to ``pennsylvaniagpugraphclustering_b200/_build/``:
 
 * ``libpggc_b200.so``   -- the CUDA kernels, the multilevel driver and the C ABI
                            declared in ``include/pggc.h``;
-* ``libpggc_graphgen.so`` -- host-side seeded synthetic graph generators.
+* ``libpggc_graphgen.so`` -- host-side seeded synthetic graph generators;
+* ``plouvain``, ``pleiden``, ``pleiden+``, ``meme``, ``verify_obj`` -- the
+  reference's command-line programs (app/CMakeLists.txt:3-7) over the C ABI.
 """
 from __future__ import annotations
 
@@ -85,10 +87,40 @@ def build_cuda(force: bool = False, verbose_ptxas: bool = False) -> str:
     return out
 
 
+APPS = {  # program: (source, extra defines); app/CMakeLists.txt:3-7, 17-19
+    "plouvain": ("cluster_main.cpp", ["-DPGGC_APP_METHOD=0"]),
+    "pleiden": ("cluster_main.cpp", ["-DPGGC_APP_METHOD=1"]),
+    "pleiden+": ("cluster_main.cpp", ["-DPGGC_APP_METHOD=2"]),
+    "meme": ("meme_main.cpp", []),
+    "verify_obj": ("verify_main.cpp", []),
+}
+
+
+def build_apps(force: bool = False) -> list[str]:
+    """Host programs linked against libpggc_b200.so (found next to them)."""
+    apps_dir = os.path.join(HERE, "apps")
+    lib = os.path.join(OUT, "libpggc_b200.so")
+    hdrs = [os.path.join(apps_dir, "app_common.hpp"), os.path.join(INCLUDE, "pggc.h")]
+    outs, jobs = [], []
+    for name, (src, defs) in APPS.items():
+        out = os.path.join(OUT, name)
+        outs.append(out)
+        srcp = os.path.join(apps_dir, src)
+        if force or _stale(out, [srcp, lib] + hdrs):
+            cmd = [_host_cxx(), "-O2", "-std=c++17", *defs, "-I", INCLUDE, "-I", apps_dir, srcp, "-o", out,
+                   "-L", OUT, "-lpggc_b200", "-Wl,-rpath,$ORIGIN", "-pthread"]
+            jobs.append(subprocess.Popen(cmd))
+    for j in jobs:
+        if j.wait() != 0:
+            raise RuntimeError("building the command-line programs failed")
+    return outs
+
+
 def build_all(force: bool = False) -> None:
     build_graphgen(force)
     if cuda_sources():
         build_cuda(force)
+        build_apps(force)
 
 
 if __name__ == "__main__":
