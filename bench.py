@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--batched-learned", type=int, default=0, metavar="K",
                     help="also time a population of K seeds run concurrently (pggc_batch_run) with the learned "
                          "move filter, trained first on logs of plain runs of smaller graphs")
+    ap.add_argument("--by-level", action="store_true",
+                    help="profiled run also splits each kernel family by multilevel level (adds 'by_level')")
     ap.add_argument("--ex-iters", type=int, default=-1,
                     help="pLeiden+ passes after the first (-1: until the objective stops rising)")
     return ap.parse_args()
@@ -242,15 +244,31 @@ def ours(args):
     # one more, untimed run with per-family CUDA events and device byte
     # counters on: the kernel breakdown and the roofline figures
     _lib.check(lib.pggc_profile_reset(mem.handle))
-    _lib.check(lib.pggc_profile_enable(mem.handle, 1))
+    _lib.check(lib.pggc_profile_enable(mem.handle, 2 if args.by_level else 1))
     step(args.seed + rank)
     _lib.check(lib.pggc_profile_enable(mem.handle, 0))
     fam = {}
-    for f in DOMINANT_FAMILIES + SUB_PHASES:
+
+    def read_family(f):
         n_l, t_ms, by = (_lib.ctypes.c_int64(), _lib.ctypes.c_double(), _lib.ctypes.c_double())
         _lib.check(lib.pggc_profile_read(mem.handle, f.encode(), _lib.ctypes.byref(n_l), _lib.ctypes.byref(t_ms),
                                          _lib.ctypes.byref(by)))
-        fam[f] = (n_l.value, t_ms.value, by.value)
+        return n_l.value, t_ms.value, by.value
+
+    for f in DOMINANT_FAMILIES + SUB_PHASES:
+        fam[f] = read_family(f)
+    by_level = None
+    if args.by_level:
+        need = _lib.ctypes.c_int64()
+        _lib.check(lib.pggc_profile_names(mem.handle, None, 0, _lib.ctypes.byref(need)))
+        buf = _lib.ctypes.create_string_buffer(need.value)
+        _lib.check(lib.pggc_profile_names(mem.handle, buf, need.value, None))
+        by_level = {}
+        for name in buf.value.decode().split("\n"):
+            if "@" in name:
+                f, lv = name.split("@", 1)
+                n_l, t_ms, _ = read_family(name)
+                by_level.setdefault(f, {})[lv] = {"launches": n_l, "ms": round(t_ms, 3)}
     q_labels = labels.cpu().numpy()
     q, _ = pg.verify_objective(mem, wg, q_labels, pg.OBJ_WMOD)
 
@@ -327,6 +345,10 @@ def ours(args):
     }
     if bl is not None:
         line["batched_learned"] = bl
+    if by_level is not None:
+        line["by_level"] = by_level
+        line["passes_profile"] = {f: {"launches": v[0], "ms": v[1]} for f, v in
+                                  ((f, read_family(f)) for f in ("pass_first", "pass_improve"))}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

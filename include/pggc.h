@@ -83,9 +83,12 @@ pggc_status pggc_debug_set_probe_limit(pggc_context* ctx, int limit);
  * EXTRA_TIMING measurements (src/clustering_methods.cpp:78-108).  Families:
  * "select_warp", "select_block", "select_huge", "afterburner_warp",
  * "afterburner_block", "own_weights", "contract", "leiden_refine", "orderings". */
-pggc_status pggc_profile_enable(pggc_context* ctx, int on);
+pggc_status pggc_profile_enable(pggc_context* ctx, int on); /* 2: also per level, "family@level" */
 pggc_status pggc_profile_reset(pggc_context* ctx);
 pggc_status pggc_profile_read(pggc_context* ctx, const char* family, int64_t* launches, double* ms, double* bytes);
+/* the recorded family names, newline-separated, into buf (cap bytes, NUL
+ * terminated); *needed = the size that holds them all */
+pggc_status pggc_profile_names(pggc_context* ctx, char* buf, int64_t cap, int64_t* needed);
 
 /* ---- memory_store (interface/memory_store.hpp:84-90) ---------------------- */
 pggc_status pggc_context_create(int device, pggc_context** out);

@@ -68,6 +68,7 @@ _SIGS = {
     "pggc_debug_set_probe_limit": (_ci, [_vp, _ci]),
     "pggc_profile_enable": (_ci, [_vp, _ci]),
     "pggc_profile_reset": (_ci, [_vp]),
+    "pggc_profile_names": (_ci, [_vp, ctypes.c_char_p, _i64, ctypes.POINTER(_i64)]),
     "pggc_profile_read": (_ci, [_vp, ctypes.c_char_p, ctypes.POINTER(_i64), ctypes.POINTER(_dbl),
                                ctypes.POINTER(_dbl)]),
     "pggc_context_create": (_ci, [_ci, _PP]),

@@ -298,6 +298,7 @@ pggc_status pggc_profile_enable(pggc_context* ctx, int on) {
         need(ctx != nullptr, "NULL context");
         ctx->ctx->prof_flush();
         ctx->ctx->profiling = on != 0;
+        ctx->ctx->prof_by_level = on == 2;
     });
 }
 
@@ -305,6 +306,24 @@ pggc_status pggc_profile_reset(pggc_context* ctx) {
     return guarded([&] {
         need(ctx != nullptr, "NULL context");
         ctx->ctx->prof_reset();
+    });
+}
+
+pggc_status pggc_profile_names(pggc_context* ctx, char* buf, int64_t cap, int64_t* needed) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL context");
+        ctx->ctx->prof_flush();
+        std::string all;
+        for (auto& kv : ctx->ctx->prof) {
+            all += kv.first;
+            all += '\n';
+        }
+        if (needed) *needed = (int64_t)all.size() + 1;
+        if (buf && cap > 0) {
+            const size_t k = std::min<size_t>(all.size(), (size_t)cap - 1);
+            std::memcpy(buf, all.data(), k);
+            buf[k] = 0;
+        }
     });
 }
 

@@ -42,7 +42,13 @@ struct Context {
     unsigned long long* d_prof = nullptr;  // [64] device byte counters
     std::map<std::string, int> prof_slot;
     std::map<std::string, ProfStat> prof;
-    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    struct ProfPending {
+        std::string family, level_key;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfPending> prof_pending;
+    bool prof_by_level = false;  // also record "family@level[@tag]" (multilevel level index)
+    const char* prof_tag = nullptr;  // e.g. which sweep of a local move
     std::vector<cudaEvent_t> ev_pool;
     // learned move filter (filter.cuh): mode 0 off, 1 log (features, label)
     // samples from plain sweeps, 2 skip the vertices the network rejects
@@ -111,8 +117,8 @@ struct Context {
             if (e.first) cudaFreeAsync(e.first, stream);
         if (arena) cudaFreeAsync(arena, stream);
         for (auto& pe : prof_pending) {
-            cudaEventDestroy(pe.second.first);
-            cudaEventDestroy(pe.second.second);
+            cudaEventDestroy(pe.a);
+            cudaEventDestroy(pe.b);
         }
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (void* q : {(void*)filt.net, (void*)filt.params, (void*)filt.log_x, (void*)filt.log_y, (void*)filt.log_v,
@@ -190,7 +196,12 @@ struct Context {
         if (profiling) prof[family].bytes += bytes;
     }
     void prof_record(const std::string& family, cudaEvent_t a, cudaEvent_t b) {
-        prof_pending.push_back({family, {a, b}});
+        std::string lk;
+        if (prof_by_level) {
+            lk = family + "@" + std::to_string(filt.level);
+            if (prof_tag) lk += std::string("@") + prof_tag;
+        }
+        prof_pending.push_back({family, std::move(lk), a, b});
         if (prof_pending.size() >= 8192) prof_flush();
     }
     void prof_flush() {
@@ -198,12 +209,17 @@ struct Context {
         sync();
         for (auto& pe : prof_pending) {
             float ms = 0.f;
-            PGGC_CUDA(cudaEventElapsedTime(&ms, pe.second.first, pe.second.second));
-            auto& st = prof[pe.first];
+            PGGC_CUDA(cudaEventElapsedTime(&ms, pe.a, pe.b));
+            auto& st = prof[pe.family];
             st.launches += 1;
             st.ms += ms;
-            ev_pool.push_back(pe.second.first);
-            ev_pool.push_back(pe.second.second);
+            if (!pe.level_key.empty()) {
+                auto& sl = prof[pe.level_key];
+                sl.launches += 1;
+                sl.ms += ms;
+            }
+            ev_pool.push_back(pe.a);
+            ev_pool.push_back(pe.b);
         }
         prof_pending.clear();
         if (!prof_slot.empty()) {

@@ -201,6 +201,16 @@ __device__ __forceinline__ V group_sum(unsigned peers, V val, bool leader) {
     return s;
 }
 
+// Sum of the weights of the lanes in `peers` (equal neighbour clusters), valid
+// at the leader: the lane-order shuffle sum, or the count for unit weights.
+template <class W>
+__device__ __forceinline__ typename Traits<W>::V peer_sum(const SelArgs<W>& a, unsigned peers, W wr, bool keep,
+                                                          bool leader) {
+    using V = typename Traits<W>::V;
+    if (!a.g.w) return V(__popc(peers));
+    return group_sum<V>(peers, keep ? V(wr) : V(0), leader);
+}
+
 // Linear-probing insert; gives up (latching DEV_ERR_PROBE) after the table size
 // or `cap` probes, whichever is smaller (cap = 0: no extra limit).
 template <class V>
@@ -234,12 +244,12 @@ __device__ __forceinline__ void chunk_to_table(const SelArgs<W>& a, const VCtx& 
     using V = typename Traits<W>::V;
     bool valid = j < e;
     i32 c = valid ? a.part[a.g.col[j]] : -1;
-    V wv = valid ? V(a.g.wgt(j)) : V(0);
+    W wr = valid ? a.g.wgt(j) : W(0);
     bool keep = valid && c != vc.p;
     i32 key = keep ? c : (i32)(0x80000000u | lane_id());
     unsigned peers = __match_any_sync(FULL, key);
     bool leader = keep && ((peers & lanemask_lt()) == 0);
-    V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
+    V s = peer_sum<W>(a, peers, wr, keep, leader);
     if (leader) table_add(keys, vals, mask, c, s, a.err, a.probe_cap);
 }
 
@@ -275,12 +285,12 @@ __device__ __forceinline__ bool chunk_to_table_try(const SelArgs<W>& a, const VC
     using V = typename Traits<W>::V;
     bool valid = j < e;
     i32 c = valid ? a.part[a.g.col[j]] : -1;
-    V wv = valid ? V(a.g.wgt(j)) : V(0);
+    W wr = valid ? a.g.wgt(j) : W(0);
     bool keep = valid && c != vc.p;
     i32 key = keep ? c : (i32)(0x80000000u | lane_id());
     unsigned peers = __match_any_sync(FULL, key);
     bool leader = keep && ((peers & lanemask_lt()) == 0);
-    V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
+    V s = peer_sum<W>(a, peers, wr, keep, leader);
     return leader ? table_try_add(keys, vals, mask, c, s) : true;
 }
 
@@ -315,12 +325,12 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, R
             i64 j = b + l;
             bool valid = j < e;
             i32 c = valid ? a.part[a.g.col[j]] : -1;
-            V wv = valid ? V(a.g.wgt(j)) : V(0);
+            W wr = valid ? a.g.wgt(j) : W(0);
             bool keep = valid && c != vc.p;
             i32 key = keep ? c : (i32)(0x80000000u | l);
             unsigned peers = __match_any_sync(FULL, key);
             bool leader = keep && ((peers & lanemask_lt()) == 0);
-            V s = a.g.w ? group_sum<V>(peers, wv, leader) : V(__popc(peers));
+            V s = peer_sum<W>(a, peers, wr, keep, leader);
             if (leader) sel_eval<W, CON>(a, vc, c, s, best);
         } else {
             u32 T = next_pow2_u32((u32)(2 * (e - b)));
@@ -487,13 +497,13 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
             }
         } else {
             i32 c[UV];
-            V wv[UV];
+            W wv[UV];
 #pragma unroll
             for (int u = 0; u < UV; u++) {
                 const i64 j = b[u] + r;
                 const bool valid = act[u] && j < e[u];
                 c[u] = valid ? a.g.col[j] : -1;
-                wv[u] = valid ? V(a.g.wgt(j)) : V(0);
+                wv[u] = valid ? a.g.wgt(j) : W(0);
             }
 #pragma unroll
             for (int u = 0; u < UV; u++) c[u] = c[u] >= 0 ? a.part[c[u]] : -1;
@@ -512,7 +522,7 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
                     peers = __match_any_sync(FULL, key);
                 }
                 bool leader = keep && ((peers & lanemask_lt()) == 0);
-                V sum = a.g.w ? group_sum<V>(peers, wv[u], leader) : V(__popc(peers));
+                V sum = peer_sum<W>(a, peers, wv[u], keep, leader);
                 if (leader) sel_eval<W, CON>(a, vc[u], c[u], sum, best);
                 group_best<G>(best);
                 if (r == 0 && act[u]) sel_finish(a, iv[u], vc[u], best);
@@ -1412,14 +1422,15 @@ __global__ void k_row_sums(DGraph<W> g, typename Traits<W>::V* out) {
     }
 }
 
+// graphs are created with their sums (make_graph) or by one context (coarse
+// levels); the lock covers a graph first used by several threads
+static std::mutex g_graph_cache_mu;
+
 template <class W>
 const typename Traits<W>::V* row_sums(Context& ctx, const Graph<W>& g) {
     using V = typename Traits<W>::V;
     if (g.n == 0) return nullptr;
-    // graphs are created with their sums (make_graph) or by one context
-    // (coarse levels); the lock covers a graph first used by several threads
-    static std::mutex mu;
-    std::lock_guard<std::mutex> lk(mu);
+    std::lock_guard<std::mutex> lk(g_graph_cache_mu);
     if (!g.rsum.p) {
         g.rsum = DBuf<V>(ctx, g.n);
         int grid = (int)std::min<i64>(ceil_div(g.n, 256), (i64)ctx.num_sms * 16);
@@ -1825,6 +1836,7 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
     const i64 n = g.n;
     if (n == 0) return;
     if (best.capacity < best.label_count) throw InvalidArg("cluster state capacity below label count");
+    ProfScope whole(ctx, strict ? "local_move_strict" : "local_move");
     Mover<W> m(ctx, g, ord, best.capacity);
     const float pm = (float)best.lambda;
     // curr_state.copy(best_state); part = best_part (src/local_mover.cpp:1365-1368)
@@ -1839,6 +1851,7 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
     copy_d2d(ctx, m.td_curr.p, best.total_deg.p, best.label_count);
     fill<i32>(ctx, m.dest.p, n, NULL_PART);
     if (!strict) m.filter_init();
+    ctx.prof_tag = "init";
     if (!is_initial) {
         m.cdata_init = true;
         own_weights_impl<W>(ctx, g, ord, m.part.p, m.pvals.p, 0, nullptr, nullptr, &m.cls);
@@ -1869,6 +1882,7 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
                 if (!budget()) break;
                 sweeps++;
                 iter_count++;
+                ctx.prof_tag = iter_count == 1 ? (enable_sa ? "sa_first" : "first") : "later";
                 m.filter_pre(iter_count - 1, best.vol_total);
                 auto a = m.sel_args(fr, !m.cdata_init, constraint, m.td_curr.p, m.part.p, m.pvals.p, m.dest.p,
                                     m.gain.p, &m.sc.p->label_count, pm);
@@ -1894,6 +1908,7 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
         for (int it = 0; it < 6; it++) {
             if (!budget()) break;
             sweeps++;
+            ctx.prof_tag = "strict";
             auto a = m.sel_args(0.0f, !m.cdata_init, constraint, m.td_curr.p, m.part.p, m.pvals.p, m.dest.p, m.gain.p,
                                 &m.sc.p->label_count, pm);
             m.label_bound_host = label_bound;
@@ -1916,12 +1931,14 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
             total_moves += nm;
         }
     }
+    ctx.prof_tag = "end";
     const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
     best.label_count = hs->best_label_count;
     best.uncut = hs->best_uncut;
     best.obj = hs->best_obj;
     ctx.check_device_error();
     m.relabel(best_part, best);
+    ctx.prof_tag = nullptr;
     if (stats) {
         stats->sweeps += sweeps;
         stats->moves += total_moves;
