@@ -535,6 +535,66 @@ __global__ void __launch_bounds__(256) k_select_grp(SelArgs<W> a, const i32* cls
     }
 }
 
+// One thread per vertex for vertices of degree <= K (classes 0 and 1): the
+// row sits in registers, equal neighbour clusters are merged by pairwise
+// compares and summed from 0 in edge order -- the order of the lane-order
+// group sum, so the gains are bit-identical -- and the best cluster is kept
+// under the same total order (gain, then smaller id).  No shuffles or match
+// instructions: the warp's 32 vertices are independent load chains.
+template <class W, bool CON, int K>
+__global__ void __launch_bounds__(256) k_select_thr(SelArgs<W> a, const i32* cls, const i64* off, int k) {
+    using V = typename Traits<W>::V;
+    const i64 lo = off[k], hi = off[k + 1];
+    unsigned long long pb = 0;
+    for (i64 x = lo + blockIdx.x * (i64)blockDim.x + threadIdx.x; x < hi; x += (i64)gridDim.x * blockDim.x) {
+        const i32 i = cls[x];
+        if (a.dest[i] == NO_MOVE) {
+            pb += sel_bytes(a, 0, false);
+            continue;
+        }
+        const VCtx vc = sel_prologue(a, i);
+        const i64 b = a.g.rowptr[i];
+        i64 e = a.g.rowptr[i + 1];
+        if (sel_no_candidate(a, i, vc)) e = b;
+        const int d = (int)(e - b);
+        pb += sel_bytes(a, d, true);
+        Best best = none_best();
+        i32 c[K];
+        W w[K];
+#pragma unroll
+        for (int t = 0; t < K; t++) {
+            c[t] = t < d ? a.g.col[b + t] : -1;
+            w[t] = t < d ? a.g.wgt(b + t) : W(0);
+        }
+        if (a.initial) {
+#pragma unroll
+            for (int t = 0; t < K; t++)
+                if (t < d) sel_eval<W, CON>(a, vc, c[t], V(w[t]), best);
+        } else {
+#pragma unroll
+            for (int t = 0; t < K; t++) c[t] = c[t] >= 0 ? a.part[c[t]] : -1;
+#pragma unroll
+            for (int t = 0; t < K; t++) {
+                bool first = c[t] >= 0 && c[t] != vc.p;
+#pragma unroll
+                for (int m = 0; m < t; m++) first = first && c[m] != c[t];
+                if (first) {
+                    V sum = V(0);
+#pragma unroll
+                    for (int m = t; m < K; m++)
+                        if (c[m] == c[t]) sum = sum + V(w[m]);
+                    sel_eval<W, CON>(a, vc, c[t], sum, best);
+                }
+            }
+        }
+        sel_finish(a, i, vc, best);
+    }
+    if (a.prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (lane_id() == 0 && pb) atomicAdd(a.prof, pb);
+    }
+}
+
 // ---- block per vertex, shared or global table -------------------------------
 // With OVF (vertices above HUGE_DEG, shared tables of gcap slots that may be
 // smaller than 2 * degree), a vertex whose distinct neighbour clusters do not
@@ -789,6 +849,60 @@ __global__ void __launch_bounds__(256) k_own_small(DGraph<W> g, const i32* lab, 
     }
 }
 
+// The canonical association of an 8-lane group after each lane r has added
+// its terms r and r + 8 from 0 (xor butterfly 4, 2, 1, read at lane 0):
+// ((a0 + a4) + (a2 + a6)) + ((a1 + a5) + (a3 + a7)).
+template <class V>
+__device__ __forceinline__ V canon_tree8(const V (&a)[8]) {
+    const V b0 = a[0] + a[4], b1 = a[1] + a[5], b2 = a[2] + a[6], b3 = a[3] + a[7];
+    return (b0 + b2) + (b1 + b3);
+}
+
+// Own-cluster weights of vertices of degree <= 16 (classes 0 and 1), one
+// thread per vertex, association of k_own_small<W, 8, 2> (canon_tree8): no
+// shuffles, 32 independent vertices per warp.
+template <class W>
+__global__ void __launch_bounds__(256) k_own_thr(DGraph<W> g, const i32* lab, typename Traits<W>::V* out, Range rg,
+                                                 int mode, unsigned char* flags, i32* dest,
+                                                 unsigned long long* prof) {
+    using V = typename Traits<W>::V;
+    const i64 lo = rg.begin(), hi = rg.end();
+    unsigned long long pb = 0;
+    for (i64 x = lo + blockIdx.x * (i64)blockDim.x + threadIdx.x; x < hi; x += (i64)gridDim.x * blockDim.x) {
+        const i32 i = rg.list[x];
+        if (mode == 1 && !flags[i]) continue;
+        const i64 b = g.rowptr[i], e = g.rowptr[i + 1];
+        const i32 li = lab[i];
+        i32 cv[16];
+        W wv[16];
+#pragma unroll
+        for (int t = 0; t < 16; t++) {
+            const bool valid = b + t < e;
+            cv[t] = valid ? g.col[b + t] : -1;
+            wv[t] = valid ? g.wgt(b + t) : W(0);
+        }
+#pragma unroll
+        for (int t = 0; t < 16; t++) cv[t] = cv[t] >= 0 ? lab[cv[t]] : -1;
+        V acc[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            acc[r] = V(0);
+            if (b + r < e) acc[r] += cv[r] == li ? V(wv[r]) : V(0);
+            if (b + r + 8 < e) acc[r] += cv[r + 8] == li ? V(wv[r + 8]) : V(0);
+        }
+        out[i] = canon_tree8<V>(acc);
+        if (mode == 1) {
+            dest[i] = NULL_PART;
+            flags[i] = 0;
+        }
+        pb += 4 + 16 + 4 + sizeof(V) + (unsigned long long)(e - b) * (8 + (g.w ? sizeof(W) : 0));
+    }
+    if (prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (lane_id() == 0 && pb) atomicAdd(prof, pb);
+    }
+}
+
 template <class W>
 void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* lab,
                       typename Traits<W>::V* out, int mode, unsigned char* flags, i32* dest,
@@ -805,9 +919,9 @@ void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, cons
     const i64 c01 = cls->count;  // host upper bound of every class range
     if (c01 > 0) {
         int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(c01, 32), (i64)ctx.num_sms * 16));
-        k_own_small<W, 8, 2><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
-                                                            dev_range(cls->list, cls->off + 0, cls->off + 2), mode,
-                                                            flags, dest, prof);
+        int grid_t = (int)std::max<i64>(1, std::min<i64>(ceil_div(c01, 256), (i64)ctx.num_sms * 16));
+        k_own_thr<W><<<grid_t, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 0, cls->off + 2),
+                                                     mode, flags, dest, prof);
         PGGC_LAUNCH_CHECK();
         k_own_small<W, 16, 2><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
                                                              dev_range(cls->list, cls->off + 2, cls->off + 3), mode,
@@ -984,6 +1098,38 @@ __global__ void __launch_bounds__(256) k_afterburner_small(ABArgs<W> a, Range rg
     if (a.prof) {
         pb = (unsigned long long)warp_sum_i64((i64)pb);
         if (l == 0 && pb) atomicAdd(a.prof, pb);
+    }
+}
+
+// Afterburner for candidates of degree <= 16, one thread per vertex, the
+// association of k_afterburner_small<W, 8, 2> (canon_tree8).
+template <class W>
+__global__ void __launch_bounds__(256) k_afterburner_thr(ABArgs<W> a, Range rg) {
+    const i64 lo = rg.begin(), hi = rg.end();
+    unsigned long long pb = 0;
+    for (i64 x = lo + blockIdx.x * (i64)blockDim.x + threadIdx.x; x < hi; x += (i64)gridDim.x * blockDim.x) {
+        const i32 i = rg.list[x];
+        const i32 best = a.dest[i];
+        if (best == NO_MOVE) continue;
+        const i32 p = a.part[i];
+        const float multi = to_f(a.g.vtx_w[i]) * a.pm;
+        const float igain = a.gain[i];
+        const i32 hv = (i32)xorshift32((u32)i);
+        const i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        double acc[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            acc[r] = 0.0;
+            if (b + r < e) acc[r] += ab_term(a, b + r, p, best, multi, igain, hv);
+            if (b + r + 8 < e) acc[r] += ab_term(a, b + r + 8, p, best, multi, igain, hv);
+        }
+        const double ch = canon_tree8<double>(acc);
+        a.keep[i] = (igain + (float)ch) >= 0.0f ? 1 : 0;
+        pb += ab_bytes(a, e - b);
+    }
+    if (a.prof) {
+        pb = (unsigned long long)warp_sum_i64((i64)pb);
+        if (lane_id() == 0 && pb) atomicAdd(a.prof, pb);
     }
 }
 
@@ -1590,11 +1736,12 @@ struct Mover {
             ProfScope ps(ctx, "select_warp");
             a.prof = ctx.prof_counter("select_warp");
             int grid_g = grid_for(ctx, ceil_div(cls.count, 32), 1, 16);
-            k_select_grp<W, CON, 8><<<grid_g, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 0);
+            int grid_t = grid_for(ctx, ceil_div(cls.count, 256), 1, 16);
+            k_select_thr<W, CON, 8><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 0);
             PGGC_LAUNCH_CHECK();
-            k_select_grp<W, CON, 16><<<grid_g, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 1);
+            k_select_thr<W, CON, 16><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 1);
             PGGC_LAUNCH_CHECK();
-            k_select_grp<W, CON, 32><<<grid_g, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 2);
+            k_select_thr<W, CON, 32><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 2);
             PGGC_LAUNCH_CHECK();
             int grid = grid_for(ctx, ceil_div(ord.off_large, SELW_WARPS), 1, 16);
             k_select_warp<W, CON><<<grid, SELW_WARPS * 32, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 3,
@@ -1672,8 +1819,8 @@ struct Mover {
             ProfScope ps(ctx, "afterburner_warp");
             if (cls.count > 0) {
                 int grid = grid_for(ctx, ceil_div(cls.count, 32), 1, 16);
-                k_afterburner_small<W, 8, 2><<<grid, 256, 0, ctx.stream>>>(
-                    a, dev_range(cls.list, cls.off + 0, cls.off + 2));
+                int grid_t = grid_for(ctx, ceil_div(cls.count, 256), 1, 16);
+                k_afterburner_thr<W><<<grid_t, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 0, cls.off + 2));
                 PGGC_LAUNCH_CHECK();
                 k_afterburner_small<W, 16, 2><<<grid, 256, 0, ctx.stream>>>(
                     a, dev_range(cls.list, cls.off + 2, cls.off + 3));
