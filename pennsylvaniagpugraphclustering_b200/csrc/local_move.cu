@@ -560,19 +560,16 @@ __global__ void __launch_bounds__(256) k_select_thr(SelArgs<W> a, const i32* cls
         pb += sel_bytes(a, d, true);
         Best best = none_best();
         i32 c[K];
-        W w[K];
 #pragma unroll
-        for (int t = 0; t < K; t++) {
-            c[t] = t < d ? a.g.col[b + t] : -1;
-            w[t] = t < d ? a.g.wgt(b + t) : W(0);
-        }
+        for (int t = 0; t < K; t++) c[t] = t < d ? a.g.col[b + t] : -1;
         if (a.initial) {
 #pragma unroll
             for (int t = 0; t < K; t++)
-                if (t < d) sel_eval<W, CON>(a, vc, c[t], V(w[t]), best);
+                if (t < d) sel_eval<W, CON>(a, vc, c[t], V(a.g.wgt(b + t)), best);
         } else {
 #pragma unroll
             for (int t = 0; t < K; t++) c[t] = c[t] >= 0 ? a.part[c[t]] : -1;
+            // weights are read where they are summed (the row is in L1)
 #pragma unroll
             for (int t = 0; t < K; t++) {
                 bool first = c[t] >= 0 && c[t] != vc.p;
@@ -582,7 +579,7 @@ __global__ void __launch_bounds__(256) k_select_thr(SelArgs<W> a, const i32* cls
                     V sum = V(0);
 #pragma unroll
                     for (int m = t; m < K; m++)
-                        if (c[m] == c[t]) sum = sum + V(w[m]);
+                        if (c[m] == c[t]) sum = sum + V(a.g.wgt(b + m));
                     sel_eval<W, CON>(a, vc, c[t], sum, best);
                 }
             }
@@ -857,11 +854,25 @@ __device__ __forceinline__ V canon_tree8(const V (&a)[8]) {
     const V b0 = a[0] + a[4], b1 = a[1] + a[5], b2 = a[2] + a[6], b3 = a[3] + a[7];
     return (b0 + b2) + (b1 + b3);
 }
+// the same for an H-lane group (H = 8 or 16): the butterfly step 8 first
+template <int H, class V>
+__device__ __forceinline__ V canon_tree(const V (&a)[H]) {
+    if constexpr (H == 8) {
+        return canon_tree8<V>(a);
+    } else {
+        static_assert(H == 16, "H is 8 or 16");
+        V b[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) b[r] = a[r] + a[r + 8];
+        return canon_tree8<V>(b);
+    }
+}
 
-// Own-cluster weights of vertices of degree <= 16 (classes 0 and 1), one
-// thread per vertex, association of k_own_small<W, 8, 2> (canon_tree8): no
-// shuffles, 32 independent vertices per warp.
-template <class W>
+// Own-cluster weights of vertices of degree <= 2H (H = 8: classes 0 and 1;
+// H = 16: class 2), one thread per vertex, the association of
+// k_own_small<W, H, 2> (canon_tree): no shuffles, 32 independent vertices
+// per warp.
+template <class W, int H>
 __global__ void __launch_bounds__(256) k_own_thr(DGraph<W> g, const i32* lab, typename Traits<W>::V* out, Range rg,
                                                  int mode, unsigned char* flags, i32* dest,
                                                  unsigned long long* prof) {
@@ -873,24 +884,20 @@ __global__ void __launch_bounds__(256) k_own_thr(DGraph<W> g, const i32* lab, ty
         if (mode == 1 && !flags[i]) continue;
         const i64 b = g.rowptr[i], e = g.rowptr[i + 1];
         const i32 li = lab[i];
-        i32 cv[16];
-        W wv[16];
+        i32 cv[2 * H];
 #pragma unroll
-        for (int t = 0; t < 16; t++) {
-            const bool valid = b + t < e;
-            cv[t] = valid ? g.col[b + t] : -1;
-            wv[t] = valid ? g.wgt(b + t) : W(0);
-        }
+        for (int t = 0; t < 2 * H; t++) cv[t] = b + t < e ? g.col[b + t] : -1;
 #pragma unroll
-        for (int t = 0; t < 16; t++) cv[t] = cv[t] >= 0 ? lab[cv[t]] : -1;
-        V acc[8];
+        for (int t = 0; t < 2 * H; t++) cv[t] = cv[t] >= 0 ? lab[cv[t]] : -1;
+        // weights are read only for own-cluster edges (the row is in L1)
+        V acc[H];
 #pragma unroll
-        for (int r = 0; r < 8; r++) {
+        for (int r = 0; r < H; r++) {
             acc[r] = V(0);
-            if (b + r < e) acc[r] += cv[r] == li ? V(wv[r]) : V(0);
-            if (b + r + 8 < e) acc[r] += cv[r + 8] == li ? V(wv[r + 8]) : V(0);
+            if (b + r < e) acc[r] += cv[r] == li ? V(g.wgt(b + r)) : V(0);
+            if (b + r + H < e) acc[r] += cv[r + H] == li ? V(g.wgt(b + r + H)) : V(0);
         }
-        out[i] = canon_tree8<V>(acc);
+        out[i] = canon_tree<H, V>(acc);
         if (mode == 1) {
             dest[i] = NULL_PART;
             flags[i] = 0;
@@ -920,12 +927,11 @@ void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, cons
     if (c01 > 0) {
         int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(c01, 32), (i64)ctx.num_sms * 16));
         int grid_t = (int)std::max<i64>(1, std::min<i64>(ceil_div(c01, 256), (i64)ctx.num_sms * 16));
-        k_own_thr<W><<<grid_t, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 0, cls->off + 2),
-                                                     mode, flags, dest, prof);
+        k_own_thr<W, 8><<<grid_t, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 0, cls->off + 2),
+                                                        mode, flags, dest, prof);
         PGGC_LAUNCH_CHECK();
-        k_own_small<W, 16, 2><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
-                                                             dev_range(cls->list, cls->off + 2, cls->off + 3), mode,
-                                                             flags, dest, prof);
+        k_own_thr<W, 16><<<grid_t, 256, 0, ctx.stream>>>(gv, lab, out, dev_range(cls->list, cls->off + 2, cls->off + 3),
+                                                         mode, flags, dest, prof);
         PGGC_LAUNCH_CHECK();
         k_own_small<W, 32, 4><<<grid, 256, 0, ctx.stream>>>(gv, lab, out,
                                                              dev_range(cls->list, cls->off + 3, cls->off + 4), mode,
@@ -1101,9 +1107,9 @@ __global__ void __launch_bounds__(256) k_afterburner_small(ABArgs<W> a, Range rg
     }
 }
 
-// Afterburner for candidates of degree <= 16, one thread per vertex, the
-// association of k_afterburner_small<W, 8, 2> (canon_tree8).
-template <class W>
+// Afterburner for candidates of degree <= 2H, one thread per vertex, the
+// association of k_afterburner_small<W, H, 2> (canon_tree).
+template <class W, int H>
 __global__ void __launch_bounds__(256) k_afterburner_thr(ABArgs<W> a, Range rg) {
     const i64 lo = rg.begin(), hi = rg.end();
     unsigned long long pb = 0;
@@ -1116,14 +1122,14 @@ __global__ void __launch_bounds__(256) k_afterburner_thr(ABArgs<W> a, Range rg) 
         const float igain = a.gain[i];
         const i32 hv = (i32)xorshift32((u32)i);
         const i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
-        double acc[8];
+        double acc[H];
 #pragma unroll
-        for (int r = 0; r < 8; r++) {
+        for (int r = 0; r < H; r++) {
             acc[r] = 0.0;
             if (b + r < e) acc[r] += ab_term(a, b + r, p, best, multi, igain, hv);
-            if (b + r + 8 < e) acc[r] += ab_term(a, b + r + 8, p, best, multi, igain, hv);
+            if (b + r + H < e) acc[r] += ab_term(a, b + r + H, p, best, multi, igain, hv);
         }
-        const double ch = canon_tree8<double>(acc);
+        const double ch = canon_tree<H, double>(acc);
         a.keep[i] = (igain + (float)ch) >= 0.0f ? 1 : 0;
         pb += ab_bytes(a, e - b);
     }
@@ -1820,10 +1826,9 @@ struct Mover {
             if (cls.count > 0) {
                 int grid = grid_for(ctx, ceil_div(cls.count, 32), 1, 16);
                 int grid_t = grid_for(ctx, ceil_div(cls.count, 256), 1, 16);
-                k_afterburner_thr<W><<<grid_t, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 0, cls.off + 2));
+                k_afterburner_thr<W, 8><<<grid_t, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 0, cls.off + 2));
                 PGGC_LAUNCH_CHECK();
-                k_afterburner_small<W, 16, 2><<<grid, 256, 0, ctx.stream>>>(
-                    a, dev_range(cls.list, cls.off + 2, cls.off + 3));
+                k_afterburner_thr<W, 16><<<grid_t, 256, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 2, cls.off + 3));
                 PGGC_LAUNCH_CHECK();
                 k_afterburner_small<W, 32, 4><<<grid, 256, 0, ctx.stream>>>(
                     a, dev_range(cls.list, cls.off + 3, cls.off + 4));
