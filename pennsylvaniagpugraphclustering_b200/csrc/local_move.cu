@@ -730,7 +730,8 @@ __global__ void __launch_bounds__(1024) k_own_massive(DGraph<W> g, const i32* la
 }
 
 // G-lane groups over a vertex range; mode 0: every vertex, mode 1: flagged
-// vertices only (also resets their dest cache and clears the flag)
+// vertices only (also resets their dest cache and clears the flag), mode 2:
+// every vertex, resetting its dest cache (a list of affected vertices)
 template <class W, int G>
 __global__ void __launch_bounds__(256) k_own_grp(DGraph<W> g, const i32* lab, typename Traits<W>::V* out, Range rg,
                                                  int mode, unsigned char* flags, i32* dest,
@@ -748,7 +749,7 @@ __global__ void __launch_bounds__(256) k_own_grp(DGraph<W> g, const i32* lab, ty
         bool act = false;
         if (x < hi) {
             i = rg.list[x];
-            act = mode == 0 || flags[i];
+            act = mode != 1 || flags[i];
         }
         i64 b = 0, e = 0;
         i32 li = 0;
@@ -763,6 +764,8 @@ __global__ void __launch_bounds__(256) k_own_grp(DGraph<W> g, const i32* lab, ty
             if (mode == 1) {
                 dest[i] = NULL_PART;
                 flags[i] = 0;
+            } else if (mode == 2) {
+                dest[i] = NULL_PART;
             }
             // list entry, offsets, own label, result; per edge column, weight, label
             pb += 4 + 16 + 4 + sizeof(V) + (unsigned long long)(e - b) * (8 + (g.w ? sizeof(W) : 0));
@@ -950,6 +953,29 @@ void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, cons
         int gb = (int)std::min<i64>(nm, (i64)ctx.num_sms * 2);
         k_own_massive<W><<<gb, 1024, 0, ctx.stream>>>(gv, lab, out, ord.order1.p + ord.off_large2, nm, mode, flags,
                                                        dest);
+        PGGC_LAUNCH_CHECK();
+    }
+}
+
+// Own-cluster weights of a device list of vertices below MASSIVE_CUTOFF (at
+// most `bound` entries, count in *d_count), warp per vertex (the 32-lane
+// canonical association, equal to the class kernels' for every degree), then
+// the flagged massive vertices; resets the dest cache of every one.
+template <class W>
+void own_weights_list(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* lab,
+                      typename Traits<W>::V* out, const i32* list, const i64* d_count, i64 bound,
+                      unsigned char* flags, i32* dest) {
+    auto gv = g.view();
+    ProfScope ps(ctx, "own_weights");
+    unsigned long long* prof = ctx.prof_counter("own_weights");
+    const int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(std::max<i64>(bound, 1), 8), (i64)ctx.num_sms * 16));
+    k_own_grp<W, 32><<<grid, 256, 0, ctx.stream>>>(gv, lab, out, Range{list, nullptr, d_count, 0, 0}, 2, nullptr, dest,
+                                                    prof);
+    PGGC_LAUNCH_CHECK();
+    const i64 nm = g.n - ord.off_large2;
+    if (nm > 0) {
+        int gb = (int)std::min<i64>(nm, (i64)ctx.num_sms * 2);
+        k_own_massive<W><<<gb, 1024, 0, ctx.stream>>>(gv, lab, out, ord.order1.p + ord.off_large2, nm, 1, flags, dest);
         PGGC_LAUNCH_CHECK();
     }
 }
@@ -1300,6 +1326,25 @@ __global__ void k_mark_affected(DGraph<W> g, const i32* moves, i64 nm, unsigned 
     }
 }
 
+// Affected vertices of a sweep (the movers and their neighbours), listed once
+// each: vertices below MASSIVE_CUTOFF go to `list` (first marker of the
+// epoch appends), massive ones are flagged for the block kernel.
+template <class W>
+__global__ void k_mark_list(DGraph<W> g, const i32* moves, i64 nm, u32* stamp, u32 epoch, i32* list, i64* cnt,
+                            unsigned char* flags) {
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    auto mark = [&](i32 v) {
+        if (g.rowptr[v + 1] - g.rowptr[v] >= MASSIVE_CUTOFF) flags[v] = 1;
+        else if (atomicExch(&stamp[v], epoch) != epoch) list[atomicAdd((unsigned long long*)cnt, 1ull)] = v;
+    };
+    for (i64 x = gw; x < nm; x += nw) {
+        const i32 i = moves[x];
+        if (lane_id() == 0) mark(i);
+        for (i64 j = g.rowptr[i] + lane_id(); j < g.rowptr[i + 1]; j += 32) mark(g.col[j]);
+    }
+}
+
 template <class V>
 struct SqIn;
 template <>
@@ -1609,6 +1654,11 @@ struct Mover {
     View<float> gain;
     View<V> pvals, pvals_clone, td_curr;
     View<unsigned char> flags, keep, has;
+    // affected-vertex list of a sweep with few moves (stamp[v] == epoch: listed)
+    View<u32> stamp;
+    View<i32> aff;
+    View<i64> aff_cnt;
+    u32 epoch = 0;
     View<LMScalars<V>> sc;
     View<i32> gkeys;
     View<V> gvals;
@@ -1620,7 +1670,8 @@ struct Mover {
     View<i32> moved_at, csize;
 
     enum Slot { S_PART, S_DEST, S_CAND, S_MOVES, S_NEWL, S_AVAIL, S_PRIO, S_GAIN, S_PV, S_PVC, S_TD, S_FLAGS, S_KEEP,
-                S_HAS, S_SC, S_GK, S_GV, S_CLS, S_CLS_OFF, S_CLS_CNT, S_MOVED_AT, S_CSIZE, S_OVF, S_OVF_CNT };
+                S_HAS, S_SC, S_GK, S_GV, S_CLS, S_CLS_OFF, S_CLS_CNT, S_MOVED_AT, S_CSIZE, S_OVF, S_OVF_CNT,
+                S_STAMP, S_AFF, S_AFF_CNT };
 
     Mover(Context& c, const Graph<W>& gr, const Ordering& o, i64 capacity)
         : ctx(c), g(gr), ord(o), n(gr.n), cap(capacity) {
@@ -1640,6 +1691,10 @@ struct Mover {
         has.p = ctx.ws_get<unsigned char>(S_HAS, cc);
         sc.p = ctx.ws_get<LMScalars<V>>(S_SC, 1);
         PGGC_CUDA(cudaMemsetAsync(flags.p, 0, nn, ctx.stream));
+        stamp.p = ctx.ws_get<u32>(S_STAMP, nn);
+        aff.p = ctx.ws_get<i32>(S_AFF, nn);
+        aff_cnt.p = ctx.ws_get<i64>(S_AFF_CNT, 1);
+        PGGC_CUDA(cudaMemsetAsync(stamp.p, 0, sizeof(u32) * nn, ctx.stream));
         build_class_lists(ctx, g.view().rowptr, ord, S_CLS, S_CLS_OFF, S_CLS_CNT, cls);
         if (ord.n_huge > 0) {
             gcap = next_pow2_u32((u32)std::min<i64>(2 * ord.max_deg, (i64)1 << 30));
@@ -1881,10 +1936,24 @@ struct Mover {
             cdata_init = true;
             own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 0, nullptr, nullptr, &cls);
             fill<i32>(ctx, dest.p, n, NULL_PART);
-        } else {
+        } else if (nm * 16 > n) {
             k_mark_affected<W><<<grid_for(ctx, ceil_div(nm, 8), 1, 16), 256, 0, ctx.stream>>>(gv, moves.p, nm, flags.p);
             PGGC_LAUNCH_CHECK();
             own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 1, flags.p, dest.p, &cls);
+        } else {
+            // few moves: list the affected vertices once and recompute only them
+            // (the same per-vertex association as the class kernels)
+            if (++epoch == 0) {
+                PGGC_CUDA(cudaMemsetAsync(stamp.p, 0, sizeof(u32) * std::max<i64>(n, 1), ctx.stream));
+                epoch = 1;
+            }
+            PGGC_CUDA(cudaMemsetAsync(aff_cnt.p, 0, sizeof(i64), ctx.stream));
+            k_mark_list<W><<<grid_for(ctx, ceil_div(nm, 8), 1, 16), 256, 0, ctx.stream>>>(gv, moves.p, nm, stamp.p,
+                                                                                         epoch, aff.p, aff_cnt.p,
+                                                                                         flags.p);
+            PGGC_LAUNCH_CHECK();
+            own_weights_list<W>(ctx, g, ord, part.p, pvals.p, aff.p, aff_cnt.p, std::min<i64>(n, nm * (1 + ord.max_deg)),
+                                flags.p, dest.p);
         }
         update_objective_dev(lambda, label_bound);
     }
