@@ -104,8 +104,7 @@ void default_vertex_weights(Context& ctx, Graph<W>& g, int objective) {
     PGGC_LAUNCH_CHECK();
     if constexpr (std::is_same<V, double>::value) {
         if (objective == OBJ_WMOD) {
-            Ordering ord;
-            generate_orderings(ctx, gv.rowptr, g.n, ord);
+            const Ordering& ord = graph_ordering<W>(ctx, g);
             i64 nm = g.n - ord.off_large2;
             if (nm > 0) {
                 k_vw_block<W><<<(int)std::min<i64>(nm, (i64)ctx.num_sms * 2), 1024, 0, ctx.stream>>>(
@@ -205,14 +204,13 @@ void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits
     if (!improve) iota<i32>(ctx, part.p, n);
     else copy_d2d(ctx, part.p, input, n);
     SplitMix64 rng(seed);
-    Ordering ord;
     MoveStats ms;
     while (true) {
         const Graph<W>& c = *levels.back();
         if ((i64)levels.size() > MAX_LEVELS) throw DeviceFault("multilevel hierarchy exceeded MAX_LEVELS");
         double old_obj = rfd.obj;
         bool init = !improve && levels.size() == 1;
-        generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        const Ordering& ord = graph_ordering<W>(ctx, c);
         ctx.filt.level = (int)levels.size() - 1;
         local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, true, false, -1, &ms);
         if (c.nnz > 100000 && old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, false, -1, &ms);
@@ -251,7 +249,7 @@ void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits
         k_project<<<vgrid(ctx, c.n), 256, 0, ctx.stream>>>(c.n, parts[i].p, parts[i + 1].p);
         PGGC_LAUNCH_CHECK();
         if (plus) {
-            generate_orderings(ctx, c.view().rowptr, c.n, ord);
+            const Ordering& ord = graph_ordering<W>(ctx, c);
             // the finest level's last local move runs unfiltered: the exact
             // sweeps that catch what the learned filter skipped
             ctx.filt.level = (int)i;
@@ -290,14 +288,13 @@ void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Trait
         PGGC_CUDA(cudaMemsetAsync(constraint.p, 0, sizeof(i32) * constraint.n, ctx.stream));
         copy_d2d(ctx, constraint.p, constraint_in, top.n);
     }
-    Ordering ord;
     MoveStats ms;
     while (true) {
         const Graph<W>& c = *levels.back();
         if ((i64)levels.size() > MAX_LEVELS) throw DeviceFault("multilevel hierarchy exceeded MAX_LEVELS");
         DBuf<i32> part(ctx, std::max<i64>(c.n, 1));
         iota<i32>(ctx, part.p, c.n);
-        generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        const Ordering& ord = graph_ordering<W>(ctx, c);
         ctx.filt.level = (int)levels.size() - 1;
         local_move<W>(ctx, c, ord, part.p, rfd, true, constrained, constrained ? constraint.p : nullptr, true, false, -1,
                       &ms);
@@ -340,7 +337,7 @@ void louvain_part(Context& ctx, const Graph<W>& top, ClusterState<typename Trait
         const Graph<W>& c = *levels[i];
         k_project<<<vgrid(ctx, c.n), 256, 0, ctx.stream>>>(c.n, parts[i].p, parts[i + 1].p);
         PGGC_LAUNCH_CHECK();
-        generate_orderings(ctx, c.view().rowptr, c.n, ord);
+        const Ordering& ord = graph_ordering<W>(ctx, c);
         ctx.filt.level = (int)i;
         ctx.filt.suspended = i == 0;
         local_move<W>(ctx, c, ord, parts[i].p, rfd, false, false, nullptr, true, false, -1, &ms);

@@ -2,6 +2,7 @@
 // state they share (weighted_graph, cluster_data, memory_store equivalents).
 #pragma once
 #include <memory>
+#include <mutex>
 #include <vector>
 #include "scan.cuh"
 
@@ -26,6 +27,18 @@ struct Ordering {
 };
 void generate_orderings(Context& ctx, const i64* rowptr, i64 n, Ordering& o);
 
+// Per-graph products that depend on the CSR alone (its ordering and degree
+// class lists), built once on first use and kept with the graph.
+struct GraphCache {
+    std::mutex mu;
+    bool ord_ok = false;
+    Ordering ord;
+    bool cls_ok = false;
+    DBuf<i32> cls_list;
+    DBuf<i64> cls_off;
+    DBuf<unsigned long long> cls_cnt;
+};
+
 // ---------------------------------------------------------------------------
 // weighted_graph (interface/weighted_graph.h:10-19), device resident
 // ---------------------------------------------------------------------------
@@ -39,6 +52,7 @@ struct Graph {
     DBuf<W> w;
     DBuf<V> vtx_w;
     mutable DBuf<V> rsum;  // row weight sums, computed on first use by the sweep
+    std::unique_ptr<GraphCache> cache{new GraphCache()};
     // borrowed (caller-owned) arrays take precedence over the owned ones
     const i64* b_rowptr = nullptr;
     const i32* b_col = nullptr;
@@ -54,6 +68,19 @@ struct Graph {
         return g;
     }
 };
+
+// the graph's ordering (generate_orderings on its CSR), built on first use
+template <class W>
+const Ordering& graph_ordering(Context& ctx, const Graph<W>& g) {
+    GraphCache& c = *g.cache;
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (!c.ord_ok) {
+        generate_orderings(ctx, g.view().rowptr, g.n, c.ord);
+        ctx.sync();  // other streams may read it next
+        c.ord_ok = true;
+    }
+    return c.ord;
+}
 
 enum ObjKind { OBJ_MOD = 0, OBJ_WMOD = 1, OBJ_CPM = 2, OBJ_NLCC = 3, OBJ_LCC = 4 };
 

@@ -422,13 +422,10 @@ __global__ void k_class_scatter(const i32* list, i64 count, const i64* rowptr, u
     }
 }
 
-// Builds the class lists of all vertices into workspace slots.
-inline void build_class_lists(Context& ctx, const i64* rowptr, const Ordering& ord, int slot_list, int slot_off,
-                              int slot_cnt, ClassLists& cl) {
+// Builds the class lists of all vertices into cl's arrays (list: ord.n
+// entries, off: NCLS + 1, cnt: 2 * NCLS).
+inline void build_class_lists_into(Context& ctx, const i64* rowptr, const Ordering& ord, ClassLists& cl) {
     cl.count = ord.n;
-    cl.list = ctx.ws_get<i32>(slot_list, std::max<i64>(cl.count, 1));
-    cl.off = ctx.ws_get<i64>(slot_off, NCLS + 1);
-    cl.cnt = ctx.ws_get<unsigned long long>(slot_cnt, 2 * NCLS);
     PGGC_CUDA(cudaMemsetAsync(cl.cnt, 0, sizeof(unsigned long long) * 2 * NCLS, ctx.stream));
     int grid = (int)std::max<i64>(1, std::min<i64>(ceil_div(std::max<i64>(cl.count, 1), 256), (i64)ctx.num_sms * 8));
     if (cl.count > 0) {
@@ -441,6 +438,30 @@ inline void build_class_lists(Context& ctx, const i64* rowptr, const Ordering& o
         k_class_scatter<<<grid, 256, 0, ctx.stream>>>(ord.order1.p, cl.count, rowptr, cl.cnt, cl.list);
         PGGC_LAUNCH_CHECK();
     }
+}
+
+// The graph's class lists (built on first use, kept with the graph).
+template <class W>
+ClassLists graph_class_lists(Context& ctx, const Graph<W>& g, const Ordering& ord) {
+    GraphCache& c = *g.cache;
+    std::lock_guard<std::mutex> lk(c.mu);
+    ClassLists cl;
+    if (!c.cls_ok) {
+        c.cls_list = DBuf<i32>(ctx, std::max<i64>(ord.n, 1));
+        c.cls_off = DBuf<i64>(ctx, NCLS + 1);
+        c.cls_cnt = DBuf<unsigned long long>(ctx, 2 * NCLS);
+        cl.list = c.cls_list.p;
+        cl.off = c.cls_off.p;
+        cl.cnt = c.cls_cnt.p;
+        build_class_lists_into(ctx, g.view().rowptr, ord, cl);
+        ctx.sync();  // other streams may read them next
+        c.cls_ok = true;
+    }
+    cl.list = c.cls_list.p;
+    cl.off = c.cls_off.p;
+    cl.cnt = c.cls_cnt.p;
+    cl.count = ord.n;
+    return cl;
 }
 
 template <int G>
@@ -923,7 +944,7 @@ void own_weights_impl(Context& ctx, const Graph<W>& g, const Ordering& ord, cons
     unsigned long long* prof = ctx.prof_counter("own_weights");
     ClassLists local;
     if (!cls) {
-        build_class_lists(ctx, gv.rowptr, ord, WS_OWN_CLS, WS_OWN_OFF, WS_OWN_CNT, local);
+        local = graph_class_lists<W>(ctx, g, ord);
         cls = &local;
     }
     const i64 c01 = cls->count;  // host upper bound of every class range
@@ -1695,7 +1716,7 @@ struct Mover {
         aff.p = ctx.ws_get<i32>(S_AFF, nn);
         aff_cnt.p = ctx.ws_get<i64>(S_AFF_CNT, 1);
         PGGC_CUDA(cudaMemsetAsync(stamp.p, 0, sizeof(u32) * nn, ctx.stream));
-        build_class_lists(ctx, g.view().rowptr, ord, S_CLS, S_CLS_OFF, S_CLS_CNT, cls);
+        cls = graph_class_lists<W>(ctx, g, ord);
         if (ord.n_huge > 0) {
             gcap = next_pow2_u32((u32)std::min<i64>(2 * ord.max_deg, (i64)1 << 30));
             i64 nb = std::min<i64>(ord.n_huge, 32);
