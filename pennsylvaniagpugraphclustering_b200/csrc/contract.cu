@@ -465,6 +465,69 @@ __global__ void __launch_bounds__(THREADS) k_place_block(const i32* list, const 
     }
 }
 
+// Rows of a coarse graph with few vertices (nc <= BM_MAX_NC): a block per
+// row sets one bit per unique column in a shared bitmap of nc bits; the rank
+// of a column is the popcount of the bits before it (a prefix over the
+// bitmap words plus the bits below it in its word), so every entry is written
+// straight to its sorted position -- O(u + nc/32) per row instead of a
+// comparison sort.
+constexpr i64 BM_MAX_NC = 262144;
+constexpr int BM_THREADS = 256;
+
+template <class W>
+__global__ void __launch_bounds__(BM_THREADS) k_place_bitmap(const i32* list, const i64* d_count, const i64* P,
+                                                            const i64* cstart, const i64* ucount, const i64* rowptr,
+                                                            const i32* skey, const typename Traits<W>::V* sval,
+                                                            i32* col, W* wout, int nwords) {
+    extern __shared__ __align__(16) u32 bm_smem[];
+    u32* bm = bm_smem;
+    u32* pre = bm_smem + nwords;
+    __shared__ u32 wsum[BM_THREADS / 32];
+    const int tid = threadIdx.x, l = lane_id(), w = tid >> 5;
+    const int per = (nwords + BM_THREADS - 1) / BM_THREADS;
+    const int w0 = min(tid * per, nwords), w1 = min(w0 + per, nwords);
+    const i64 count = *d_count;
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        const i32 c = list[x];
+        const i64 src = P[cstart[c]];
+        const i64 u = ucount[c];
+        const i64 dst = rowptr[c];
+        for (int s = tid; s < nwords; s += BM_THREADS) bm[s] = 0u;
+        __syncthreads();
+        for (i64 s = tid; s < u; s += BM_THREADS) {
+            const u32 k = (u32)skey[src + s];
+            atomicOr(&bm[k >> 5], 1u << (k & 31));
+        }
+        __syncthreads();
+        // exclusive prefix of the word popcounts: thread chunks, then a block scan
+        u32 local = 0;
+        for (int q = w0; q < w1; q++) local += (u32)__popc(bm[q]);
+        u32 incl = local;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const u32 t = __shfl_up_sync(FULL, incl, d);
+            if (l >= d) incl += t;
+        }
+        if (l == 31) wsum[w] = incl;
+        __syncthreads();
+        u32 base = 0;
+        for (int q = 0; q < w; q++) base += wsum[q];
+        u32 run = base + incl - local;
+        for (int q = w0; q < w1; q++) {
+            pre[q] = run;
+            run += (u32)__popc(bm[q]);
+        }
+        __syncthreads();
+        for (i64 s = tid; s < u; s += BM_THREADS) {
+            const u32 k = (u32)skey[src + s];
+            const u32 r = pre[k >> 5] + (u32)__popc(bm[k >> 5] & ((1u << (k & 31)) - 1u));
+            col[dst + r] = (i32)k;
+            wout[dst + r] = to_w<W>(sval[src + s]);
+        }
+        __syncthreads();
+    }
+}
+
 // big rows: gather into (row-major) temp with composite keys, radix sort, place
 template <class V>
 __global__ void k_big_gather(const i32* list, i64 count, const i64* tstart, const i64* P, const i64* cstart,
@@ -758,27 +821,44 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
                                                       oval.p, cg->col.p, cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
-    if (p_r > 0) {
+    const bool bitmap = nc <= BM_MAX_NC;
+    if (bitmap) {
+        // every row above 32 entries: bitmap ranks (lists pr, pb, pb2, ph)
+        const int nwords = (int)ceil_div(nc, 32);
+        const size_t smem = sizeof(u32) * 2 * (size_t)nwords;
+        set_dynamic_smem_once(k_place_bitmap<W>, (int)(sizeof(u32) * 2 * ceil_div(BM_MAX_NC, 32)), ctx.device);
+        const i64 lists[4] = {p_r, p_b, p_b2, p_h};
+        i32* lp[4] = {pr.p, pb.p, pb2.p, ph.p};
+        for (int q = 0; q < 4; q++) {
+            if (lists[q] <= 0) continue;
+            int grid = (int)std::min<i64>(lists[q], (i64)ctx.num_sms * 4);
+            k_place_bitmap<W><<<grid, BM_THREADS, smem, ctx.stream>>>(lp[q], counts.p + 8 + q, P.p, cstart.p, ucount.p,
+                                                                     cg->rowptr.p, okey.p, oval.p, cg->col.p,
+                                                                     cg->w.p, nwords);
+            PGGC_LAUNCH_CHECK();
+        }
+    }
+    if (!bitmap && p_r > 0) {
         int grid = (int)std::min<i64>(ceil_div(p_r, PW_WARPS), (i64)ctx.num_sms * 8);
         k_place_warp_rank<W><<<grid, PW_WARPS * 32, 0, ctx.stream>>>(pr.p, counts.p + 8, P.p, cstart.p, ucount.p,
                                                                      cg->rowptr.p, okey.p, oval.p, cg->col.p,
                                                                      cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
-    if (p_b > 0) {
+    if (!bitmap && p_b > 0) {
         int grid = (int)std::min<i64>(p_b, (i64)ctx.num_sms * 8);
         k_place_block<W, 256, PB_MID><<<grid, 256, 0, ctx.stream>>>(pb.p, counts.p + 9, P.p, cstart.p, ucount.p,
                                                                     cg->rowptr.p, okey.p, oval.p, cg->col.p, cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
-    if (p_b2 > 0) {
+    if (!bitmap && p_b2 > 0) {
         int grid = (int)std::min<i64>(p_b2, (i64)ctx.num_sms * 2);
         k_place_block<W, 1024, PB_MAX><<<grid, 1024, 0, ctx.stream>>>(pb2.p, counts.p + 10, P.p, cstart.p, ucount.p,
                                                                       cg->rowptr.p, okey.p, oval.p, cg->col.p,
                                                                       cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
-    if (p_h > 0) {
+    if (!bitmap && p_h > 0) {
         WsBuf<u64> tk(ctx, CS_TK, tn), tk2(ctx, CS_TK2, tn);
         WsBuf<V> tv(ctx, CS_TV, tn), tv2(ctx, CS_TV2, tn);
         int grid = (int)std::min<i64>(p_h, (i64)ctx.num_sms * 4);

@@ -115,3 +115,12 @@ def with_vertex_weights(hg, seed):
     else:
         g.vw = rng.integers(1, 21, hg.n).astype(np.int64)
     return g
+
+
+def symmetric_weights(hg):
+    """FP32 weights in [0.5, 1.5) from a hash of the unordered pair (equal in
+    both directions)."""
+    src = np.repeat(np.arange(hg.n, dtype=np.int64), np.diff(hg.rowptr))
+    dst = hg.col.astype(np.int64)
+    lo, hi = np.minimum(src, dst), np.maximum(src, dst)
+    return (0.5 + ((lo * 1000003 + hi * 7919) % 1000) / 1000.0).astype(np.float32)

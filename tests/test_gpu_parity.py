@@ -327,3 +327,27 @@ def test_int_weighted_lcc_louvain(mem):
     lg, sg = pg.run_clustering(mem, wg, cd_g, method=pg.METHOD_LOUVAIN, ex_iters=0, seed=7)
     assert np.array_equal(lo, lg)
     assert so.objective == sg["objective"] and so.label_count == sg["label_count"]
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_build_coarse_graph_above_bitmap_limit(mem, weighted):
+    """More coarse vertices than the shared-bitmap placement covers (262,144):
+    the comparison-sort placement kernels (register, warp rank, block bitonic,
+    radix for long rows) against the oracle."""
+    hg = G.small_rmat(seed=4, scale=19)
+    if weighted:
+        hg = G.HostGraph(hg.rowptr, hg.col, G.symmetric_weights(hg), name="rmat19w")
+    obj = pg.OBJ_WMOD if weighted else pg.OBJ_MOD
+    og, wg = _pair(mem, hg, obj)
+    for nc, seed in ((300000, 1), (270000, 2)):
+        vcmap = _random_map(hg.n, nc, seed)
+        # a few heavy coarse vertices: rows long enough for the block and radix paths
+        vcmap[: hg.n // 64] = np.arange(hg.n // 64, dtype=np.int32) % 8
+        co = O.build_coarse_graph(og, vcmap, nc)
+        cg = pg.build_coarse_graph(mem, wg, vcmap, nc)
+        ro, col_o, w_o, vw_o = co.arrays()
+        rg, col_g, w_g, vw_g = cg.to_host()
+        assert np.array_equal(ro, rg)
+        assert np.array_equal(col_o, col_g)
+        assert np.array_equal(w_o, w_g)
+        assert np.array_equal(vw_o, vw_g)
