@@ -107,6 +107,7 @@ struct SelArgs {
     const i64* label_count;  // device
     const V* rsum;           // row weight sums (NULL: no bound check)
     int keys32;              // cluster ids < 2^29: group match keys fit 32 bits
+    int dense;               // block kernels: every label indexes the shared table directly
     float pm;
     float fr;
     int initial;
@@ -647,6 +648,29 @@ __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg
         if (a.initial) {
             for (i64 j = b + threadIdx.x; j < e; j += THREADS)
                 sel_eval<W, CON>(a, vc, a.g.col[j], V(a.g.wgt(j)), best);
+        } else if (!GLOBAL && a.dense) {
+            // dense table: slot = cluster id (every label fits the shared
+            // table); a cluster is present when its weight sum is positive,
+            // the only sums sel_eval accepts
+            const i64 L = *a.label_count;
+            for (i64 s = threadIdx.x; s < L; s += THREADS) vals[s] = V(0);
+            __syncthreads();
+            for (i64 j = b + (i64)w * 32 + l; j - l < e; j += THREADS) {
+                const bool valid = j < e;
+                const i32 c = valid ? a.part[a.g.col[j]] : -1;
+                const W wr = valid ? a.g.wgt(j) : W(0);
+                const bool keep = valid && c != vc.p;
+                const i32 key = keep ? c : (i32)(0x80000000u | l);
+                const unsigned peers = __match_any_sync(FULL, key);
+                const bool leader = keep && ((peers & lanemask_lt()) == 0);
+                const V sum = peer_sum<W>(a, peers, wr, keep, leader);
+                if (leader) vatomic_add(&vals[c], sum);
+            }
+            __syncthreads();
+            for (i64 s = threadIdx.x; s < L; s += THREADS) {
+                const V x = vals[s];
+                if (x > V(0)) sel_eval<W, CON>(a, vc, (i32)s, x, best);
+            }
         } else {
             i64 U = min(e - b, *a.label_count);
             u32 T = next_pow2_u32((u32)(2 * U));
@@ -1807,6 +1831,7 @@ struct Mover {
         a.prof = nullptr;
         a.probe_cap = ctx.probe_cap;
         a.keys32 = cap < ((i64)1 << 29) ? 1 : 0;
+        a.dense = 0;
         return a;
     }
 
@@ -1838,13 +1863,19 @@ struct Mover {
             // class 5 (degree <= 4096): 8192-slot tables, 2 blocks of 512 per SM
             const size_t slot = sizeof(V) + sizeof(i32);
             const i64 n4 = std::min<i64>(nb, (i64)ctx.num_sms * 8), n5 = std::min<i64>(nb, (i64)ctx.num_sms * 2);
+            // with at most as many labels as table slots, the table is indexed
+            // by cluster id directly (no probing, no keys)
+            SelArgs<W> a4 = a;
+            a4.dense = label_bound_host <= 2048 ? 1 : 0;
             k_select_block<W, CON, false, 256><<<(int)n4, 256, slot * 2048, ctx.stream>>>(
-                a, dev_range(cls.list, cls.off + 4, cls.off + 5), nullptr, nullptr, 2048);
+                a4, dev_range(cls.list, cls.off + 4, cls.off + 5), nullptr, nullptr, 2048);
             PGGC_LAUNCH_CHECK();
             if (ord.max_deg > 1024) {
+                SelArgs<W> a5 = a;
+                a5.dense = label_bound_host <= SEL_TS_MAX ? 1 : 0;
                 set_dynamic_smem_once(k_select_block<W, CON, false, 512>, (int)(slot * SEL_TS_MAX), ctx.device);
                 k_select_block<W, CON, false, 512><<<(int)n5, 512, slot * SEL_TS_MAX, ctx.stream>>>(
-                    a, dev_range(cls.list, cls.off + 5, cls.off + 6), nullptr, nullptr, SEL_TS_MAX);
+                    a5, dev_range(cls.list, cls.off + 5, cls.off + 6), nullptr, nullptr, SEL_TS_MAX);
                 PGGC_LAUNCH_CHECK();
             }
         }
@@ -1860,8 +1891,10 @@ struct Mover {
             PGGC_CUDA(cudaMemsetAsync(ovf_cnt, 0, sizeof(i64), ctx.stream));
             set_dynamic_smem_once(k_select_block<W, CON, false, 1024, true>, (int)(slot * TS), ctx.device);
             int grid = (int)std::min<i64>(ord.n_huge, (i64)ctx.num_sms);
+            SelArgs<W> ah = a;
+            ah.dense = label_bound_host <= TS ? 1 : 0;
             k_select_block<W, CON, false, 1024, true><<<grid, 1024, slot * TS, ctx.stream>>>(
-                a, host_range(ord.huge.p, 0, ord.n_huge), nullptr, nullptr, TS, ovf, ovf_cnt);
+                ah, host_range(ord.huge.p, 0, ord.n_huge), nullptr, nullptr, TS, ovf, ovf_cnt);
             PGGC_LAUNCH_CHECK();
             int ggrid = (int)std::min<i64>(ord.n_huge, 32);
             k_select_block<W, CON, true><<<ggrid, 256, 0, ctx.stream>>>(a, Range{ovf, nullptr, ovf_cnt, 0, 0}, gkeys.p,
