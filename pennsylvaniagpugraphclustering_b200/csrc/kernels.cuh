@@ -69,6 +69,71 @@ struct Graph {
     }
 };
 
+// A slice of a vertex list whose bounds live on the host or in device memory.
+struct Range {
+    const i32* list;
+    const i64* d_lo;
+    const i64* d_hi;
+    i64 lo, hi;
+    __device__ __forceinline__ i64 begin() const { return d_lo ? *d_lo : lo; }
+    __device__ __forceinline__ i64 end() const { return d_hi ? *d_hi : hi; }
+};
+inline Range host_range(const i32* list, i64 lo, i64 hi) { return Range{list, nullptr, nullptr, lo, hi}; }
+inline Range dev_range(const i32* list, const i64* d_lo, const i64* d_hi) { return Range{list, d_lo, d_hi, 0, 0}; }
+
+// Degree classes of the sweep kernels: 0 (<= 8), 1 (<= 16), 2 (<= 32),
+// 3 (< 128), 4 (<= 1024), 5 (<= 4096), 6 (above); the class lists hold every
+// vertex grouped by class.
+constexpr int NCLS = 7;
+struct ClassLists {
+    i32* list = nullptr;                // [count] vertices grouped by class
+    i64* off = nullptr;                 // [NCLS + 1] device class offsets
+    unsigned long long* cnt = nullptr;  // [2 * NCLS] device counters / cursors
+    i64 count = 0;                      // host: number of listed vertices
+};
+// the graph's class lists (built on first use, kept with the graph)
+template <class W>
+ClassLists graph_class_lists(Context& ctx, const Graph<W>& g, const Ordering& ord);
+
+// The canonical association of an 8-lane group after each lane r has added
+// its terms r and r + 8 from 0 (xor butterfly 4, 2, 1, read at lane 0):
+// ((a0 + a4) + (a2 + a6)) + ((a1 + a5) + (a3 + a7)).
+template <class V>
+__device__ __forceinline__ V canon_tree8(const V (&a)[8]) {
+    const V b0 = a[0] + a[4], b1 = a[1] + a[5], b2 = a[2] + a[6], b3 = a[3] + a[7];
+    return (b0 + b2) + (b1 + b3);
+}
+// the same for an H-lane group (H = 8 or 16): the butterfly step 8 first
+template <int H, class V>
+__device__ __forceinline__ V canon_tree(const V (&a)[H]) {
+    if constexpr (H == 8) {
+        return canon_tree8<V>(a);
+    } else {
+        static_assert(H == 16, "H is 8 or 16");
+        V b[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) b[r] = a[r] + a[r + 8];
+        return canon_tree8<V>(b);
+    }
+}
+
+
+// Canonical per-vertex sum of term(j) over [b, e) with e - b <= 2H (H = 8 or
+// 16) by one thread: lane r of an H-lane group adds terms r and r + H from 0,
+// then the xor butterfly -- the 32-lane canonical association for these
+// degrees.
+template <int H, class V, class F>
+__device__ __forceinline__ V thread_vsum(i64 b, i64 e, F term) {
+    V acc[H];
+#pragma unroll
+    for (int r = 0; r < H; r++) {
+        acc[r] = V(0);
+        if (b + r < e) acc[r] += term(b + r);
+        if (b + r + H < e) acc[r] += term(b + r + H);
+    }
+    return canon_tree<H, V>(acc);
+}
+
 // the graph's ordering (generate_orderings on its CSR), built on first use
 template <class W>
 const Ordering& graph_ordering(Context& ctx, const Graph<W>& g) {

@@ -63,17 +63,6 @@ __device__ __forceinline__ void reduce_best(Best& b, unsigned mask) {
 }
 __device__ __forceinline__ void warp_best(Best& b) { reduce_best(b, FULL); }
 
-// A slice of a vertex list whose bounds live on the host or in device memory.
-struct Range {
-    const i32* list;
-    const i64* d_lo;
-    const i64* d_hi;
-    i64 lo, hi;
-    __device__ __forceinline__ i64 begin() const { return d_lo ? *d_lo : lo; }
-    __device__ __forceinline__ i64 end() const { return d_hi ? *d_hi : hi; }
-};
-inline Range host_range(const i32* list, i64 lo, i64 hi) { return Range{list, nullptr, nullptr, lo, hi}; }
-inline Range dev_range(const i32* list, const i64* d_lo, const i64* d_hi) { return Range{list, d_lo, d_hi, 0, 0}; }
 
 // canonical per-vertex sum by a G-lane group (exact match of the 32-lane
 // association for degree <= 2G; integer sums are order-free)
@@ -362,17 +351,10 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, R
 // a warp can serve 4, 2 or 1 low-degree vertices at once and the block
 // kernels get shared tables sized to their class (2048 or 8192 slots).  Order
 // inside a class is irrelevant: every consumer treats vertices independently.
-constexpr int NCLS = 7;
 __device__ __forceinline__ int deg_class(i64 d) {
     return d <= 8 ? 0 : d <= 16 ? 1 : d <= 32 ? 2 : d < LARGE_CUTOFF ? 3 : d <= 1024 ? 4 : d <= HUGE_DEG ? 5 : 6;
 }
 
-struct ClassLists {
-    i32* list = nullptr;          // [count] vertices grouped by class
-    i64* off = nullptr;           // [NCLS + 1] device class offsets
-    unsigned long long* cnt = nullptr;  // [2 * NCLS] device counters / cursors
-    i64 count = 0;                // host: number of listed vertices
-};
 
 __global__ void k_class_count(const i32* list, i64 count, const i64* rowptr, unsigned long long* cnt) {
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
@@ -891,28 +873,6 @@ __global__ void __launch_bounds__(256) k_own_small(DGraph<W> g, const i32* lab, 
     if (prof) {
         pb = (unsigned long long)warp_sum_i64((i64)pb);
         if (l == 0 && pb) atomicAdd(prof, pb);
-    }
-}
-
-// The canonical association of an 8-lane group after each lane r has added
-// its terms r and r + 8 from 0 (xor butterfly 4, 2, 1, read at lane 0):
-// ((a0 + a4) + (a2 + a6)) + ((a1 + a5) + (a3 + a7)).
-template <class V>
-__device__ __forceinline__ V canon_tree8(const V (&a)[8]) {
-    const V b0 = a[0] + a[4], b1 = a[1] + a[5], b2 = a[2] + a[6], b3 = a[3] + a[7];
-    return (b0 + b2) + (b1 + b3);
-}
-// the same for an H-lane group (H = 8 or 16): the butterfly step 8 first
-template <int H, class V>
-__device__ __forceinline__ V canon_tree(const V (&a)[H]) {
-    if constexpr (H == 8) {
-        return canon_tree8<V>(a);
-    } else {
-        static_assert(H == 16, "H is 8 or 16");
-        V b[8];
-#pragma unroll
-        for (int r = 0; r < 8; r++) b[r] = a[r] + a[r + 8];
-        return canon_tree8<V>(b);
     }
 }
 
@@ -2241,6 +2201,7 @@ i64 select_pass(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32*
 }
 
 #define PGGC_INST_LM(W)                                                                                             \
+    template ClassLists graph_class_lists<W>(Context&, const Graph<W>&, const Ordering&);                           \
     template void local_move<W>(Context&, const Graph<W>&, const Ordering&, i32*, ClusterState<Traits<W>::V>&, bool, \
                                 bool, i32*, bool, bool, int, MoveStats*);                                           \
     template i64 select_pass<W>(Context&, const Graph<W>&, const Ordering&, const i32*, const Traits<W>::V*,         \
