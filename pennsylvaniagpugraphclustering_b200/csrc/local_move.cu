@@ -1336,11 +1336,11 @@ __global__ void k_mark_affected(DGraph<W> g, const i32* moves, i64 nm, unsigned 
 // epoch appends), massive ones are flagged for the block kernel.
 template <class W>
 __global__ void k_mark_list(DGraph<W> g, const i32* moves, i64 nm, u32* stamp, u32 epoch, i32* list, i64* cnt,
-                            unsigned char* flags) {
+                            unsigned char* flags, int has_massive) {
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
     auto mark = [&](i32 v) {
-        if (g.rowptr[v + 1] - g.rowptr[v] >= MASSIVE_CUTOFF) flags[v] = 1;
+        if (has_massive && g.rowptr[v + 1] - g.rowptr[v] >= MASSIVE_CUTOFF) flags[v] = 1;
         else if (atomicExch(&stamp[v], epoch) != epoch) list[atomicAdd((unsigned long long*)cnt, 1ull)] = v;
     };
     for (i64 x = gw; x < nm; x += nw) {
@@ -1613,14 +1613,23 @@ inline int grid_for(Context& ctx, i64 work, int per_block, int max_per_sm = 16) 
     return (int)std::max<i64>(1, std::min<i64>(ceil_div(std::max<i64>(work, 1), per_block), (i64)ctx.num_sms * max_per_sm));
 }
 
-// Row weight sums (one thread per vertex; computed once per graph)
+// Row weight sums (8-lane groups per vertex; computed once per graph).  Only
+// the no-candidate bound reads them, whose one-FP32-step margin covers any
+// summation order.
 template <class W>
 __global__ void k_row_sums(DGraph<W> g, typename Traits<W>::V* out) {
     using V = typename Traits<W>::V;
-    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < g.n; i += (i64)gridDim.x * blockDim.x) {
+    const int r = lane_id() & 7;
+    const i64 gg = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 3;
+    const i64 ng = ((i64)gridDim.x * blockDim.x) >> 3;
+    for (i64 base = gg - (gg & 3); base < g.n; base += ng) {
+        const i64 i = base + (gg & 3);
         V s = V(0);
-        for (i64 j = g.rowptr[i]; j < g.rowptr[i + 1]; j++) s += V(g.wgt(j));
-        out[i] = s;
+        if (i < g.n)
+            for (i64 j = g.rowptr[i] + r; j < g.rowptr[i + 1]; j += 8) s += V(g.wgt(j));
+#pragma unroll
+        for (int d = 4; d >= 1; d >>= 1) s = s + __shfl_xor_sync(FULL, s, d);
+        if (r == 0 && i < g.n) out[i] = s;
     }
 }
 
@@ -1635,8 +1644,8 @@ const typename Traits<W>::V* row_sums(Context& ctx, const Graph<W>& g) {
     std::lock_guard<std::mutex> lk(g_graph_cache_mu);
     if (!g.rsum.p) {
         g.rsum = DBuf<V>(ctx, g.n);
-        int grid = (int)std::min<i64>(ceil_div(g.n, 256), (i64)ctx.num_sms * 16);
-        k_row_sums<W><<<grid, 256, 0, ctx.stream>>>(g.view(), g.rsum.p);
+        k_row_sums<W><<<(int)std::min<i64>(ceil_div(g.n, 32), (i64)ctx.num_sms * 16), 256, 0, ctx.stream>>>(g.view(),
+                                                                                                          g.rsum.p);
         PGGC_LAUNCH_CHECK();
     }
     return g.rsum.p;
@@ -1964,7 +1973,7 @@ struct Mover {
             PGGC_CUDA(cudaMemsetAsync(aff_cnt.p, 0, sizeof(i64), ctx.stream));
             k_mark_list<W><<<grid_for(ctx, ceil_div(nm, 8), 1, 16), 256, 0, ctx.stream>>>(gv, moves.p, nm, stamp.p,
                                                                                          epoch, aff.p, aff_cnt.p,
-                                                                                         flags.p);
+                                                                                         flags.p, ord.off_large2 < n);
             PGGC_LAUNCH_CHECK();
             own_weights_list<W>(ctx, g, ord, part.p, pvals.p, aff.p, aff_cnt.p, std::min<i64>(n, nm * (1 + ord.max_deg)),
                                 flags.p, dest.p);
