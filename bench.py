@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--batched-learned", type=int, default=0, metavar="K",
                     help="also time a population of K seeds run concurrently (pggc_batch_run) with the learned "
                          "move filter, trained first on logs of plain runs of smaller graphs")
+    ap.add_argument("--recall", type=float, default=0.98,
+                    help="--batched-learned: recall on the training logs that sets the filter threshold")
     ap.add_argument("--by-level", action="store_true",
                     help="profiled run also splits each kernel family by multilevel level (adds 'by_level')")
     ap.add_argument("--ex-iters", type=int, default=-1,
@@ -377,7 +379,7 @@ def batched_learned(args, pg, mem, wg, m, q_plain):
     y = np.concatenate(ys)
     pos_w = float(min(20.0, (len(y) - y.sum()) / max(y.sum(), 1.0)))
     params, losses = MF.train(mem, MF.init_params(1), x, y, epochs=6, batch=4096, lr=3e-3, pos_weight=pos_w)
-    thr = MF.threshold_for_recall(mem, params, x, y, recall=0.98)
+    thr = MF.threshold_for_recall(mem, params, x, y, recall=args.recall)
     train_s = time.perf_counter() - t0
     K = args.batched_learned
 
@@ -405,7 +407,7 @@ def batched_learned(args, pg, mem, wg, m, q_plain):
                 "sweeps_mean": statistics.mean(st["sweeps"] for _, st in res),
                 "filter_skipped_frac": (sk / max(ev + sk, 1)) if learned else 0.0}
 
-    out = {"unit": UNIT, "population": K, "streams": K, "plain_modularity": q_plain,
+    out = {"unit": UNIT, "population": K, "streams": K, "recall": args.recall, "plain_modularity": q_plain,
            "train_rows": int(len(y)), "train_seconds": train_s, "final_train_loss": float(losses[-1]),
            "threshold_logit": thr, "timing": "host wall clock around pggc_batch_run (all streams joined)"}
     out["learned_1"] = timed(1, True)

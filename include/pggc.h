@@ -219,7 +219,10 @@ pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_clu
  * mem_kind), stats and status.  A learned filter enabled on `ctx` applies to
  * every job.  Returns the first failing job's status (its message in
  * pggc_last_error) or PGGC_OK.  Results equal those of sequential
- * pggc_run_clustering calls with the same arguments. */
+ * pggc_run_clustering calls with the same arguments.  `streams` is an upper
+ * bound: one stream per 32 Mi directed edges of the largest graph is used
+ * (concurrent runs on graphs that fill the device are slower than sequential
+ * ones). */
 typedef struct pggc_batch_job {
     const pggc_graph* graph;
     int objective;

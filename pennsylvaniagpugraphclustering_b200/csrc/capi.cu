@@ -881,7 +881,16 @@ pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t coun
         need(c.filt.mode != 1, "sample logging is not supported in batched runs");
         if (count == 0) return;
         c.sync();
-        const int nw = (int)std::min<i64>(streams, count);
+        // Runs on large graphs already fill the device; concurrent ones then
+        // contend for L2 and the launch path and were measured slower than
+        // sequential ones (4 x pLeiden+ on a 78M-edge graph: 0.78x).  One
+        // stream per BATCH_EDGES directed edges of the largest graph.
+        constexpr i64 BATCH_EDGES = (i64)32 << 20;
+        i64 max_nnz = 1;
+        for (i64 k = 0; k < count; k++)
+            max_nnz = std::max<i64>(max_nnz, jobs[k].graph->is_float() ? jobs[k].graph->gf->nnz : jobs[k].graph->gi->nnz);
+        const i64 by_size = std::max<i64>(1, BATCH_EDGES / max_nnz);
+        const int nw = (int)std::min<i64>(std::min<i64>(streams, count), by_size);
         {
             std::lock_guard<std::mutex> lk(ctx->workers_mu);
             while ((int)ctx->workers.size() < nw) ctx->workers.push_back(std::make_unique<Context>(c.device));
