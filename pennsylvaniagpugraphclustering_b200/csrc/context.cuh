@@ -47,6 +47,11 @@ struct Context {
         cudaEvent_t a, b;
     };
     std::vector<ProfPending> prof_pending;
+    // own-cluster weights of the last local move's best state (graph uid,
+    // device array, vertex count); uid 0: none
+    unsigned long long pv_uid = 0;
+    const void* pv_ptr = nullptr;
+    long long pv_n = 0;
     bool prof_by_level = false;  // also record "family@level[@tag]" (multilevel level index)
     const char* prof_tag = nullptr;  // e.g. which sweep of a local move
     std::vector<cudaEvent_t> ev_pool;

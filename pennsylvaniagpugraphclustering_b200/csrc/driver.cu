@@ -194,7 +194,7 @@ inline int vgrid(Context& ctx, i64 n) { return (int)std::max<i64>(1, std::min<i6
 // leiden_part<plus,improve> (src/clustering_methods.cpp:47-137)
 template <class W>
 void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool plus, bool improve,
-                 const i32* input, u64 seed, i32* labels_out, RunStats* st) {
+                 const i32* input, u64 seed, i32* labels_out, RunStats* st, bool input_is_last) {
     std::vector<std::unique_ptr<Graph<W>>> coarse;
     std::vector<const Graph<W>*> levels;
     std::vector<DBuf<i32>> parts;
@@ -212,9 +212,13 @@ void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits
         bool init = !improve && levels.size() == 1;
         const Ordering& ord = graph_ordering<W>(ctx, c);
         ctx.filt.level = (int)levels.size() - 1;
-        local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, true, false, -1, &ms);
-        if (c.nnz > 100000 && old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, false, -1, &ms);
-        if (old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, true, -1, &ms);
+        // the level's later local moves (and the refinement) start from the
+        // previous local move's output: its own-cluster weights are reused
+        local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, true, false, -1, &ms,
+                      levels.size() == 1 && improve && input_is_last);
+        if (c.nnz > 100000 && old_obj == rfd.obj)
+            local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, false, -1, &ms, true);
+        if (old_obj == rfd.obj) local_move<W>(ctx, c, ord, part.p, rfd, init, false, nullptr, false, true, -1, &ms, true);
         if (rfd.label_count == c.n) {
             parts.push_back(std::move(part));
             break;
@@ -222,7 +226,7 @@ void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits
         u32 s_pick = (u32)rng.next();
         u32 s_order = (u32)rng.next();
         DBuf<i32> cmap(ctx, std::max<i64>(c.n, 1));
-        i64 nc = coarsen_leidenR<W>(ctx, c, ord, part.p, rfd, s_pick, s_order, cmap.p);
+        i64 nc = coarsen_leidenR<W>(ctx, c, ord, part.p, rfd, s_pick, s_order, cmap.p, true);
         if (nc < c.n) {
             auto next = build_coarse_graph<W>(ctx, c, cmap.p, nc);
             coarsen_vtx_w<W>(ctx, c, cmap.p, *next);
@@ -367,7 +371,8 @@ void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Trait
         } else {
             u64 s = seed + 0x9E3779B97F4A7C15ull * pass;
             pass++;
-            leiden_part<W>(ctx, g, cs, method == METHOD_LEIDEN_PLUS, improve, con.p, s, part.p, &r1);
+            // an improvement pass starts from the previous pass's output
+            leiden_part<W>(ctx, g, cs, method == METHOD_LEIDEN_PLUS, improve, con.p, s, part.p, &r1, improve);
         }
         acc.levels = r1.levels;
         acc.total_nnz = r1.total_nnz;
@@ -398,7 +403,7 @@ void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Trait
     template void run_clustering<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, int, int, u64, i32*,      \
                                     RunStats*);                                                                       \
     template void leiden_part<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, bool, bool, const i32*, u64, \
-                                 i32*, RunStats*);                                                                    \
+                                 i32*, RunStats*, bool);                                                              \
     template void louvain_part<W>(Context&, const Graph<W>&, ClusterState<Traits<W>::V>&, bool, const i32*, i32*,     \
                                   RunStats*);                                                                         \
     template void make_cluster_state<W>(Context&, const Graph<W>&, int, double, ClusterState<Traits<W>::V>&);         \

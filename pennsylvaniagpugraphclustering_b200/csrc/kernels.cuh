@@ -1,6 +1,7 @@
 // kernels.cuh -- host-side entry points of the kernel families and the device
 // state they share (weighted_graph, cluster_data, memory_store equivalents).
 #pragma once
+#include <atomic>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -27,6 +28,11 @@ struct Ordering {
 };
 void generate_orderings(Context& ctx, const i64* rowptr, i64 n, Ordering& o);
 
+inline u64 next_graph_uid() {
+    static std::atomic<u64> n{0};
+    return ++n;
+}
+
 // Per-graph products that depend on the CSR alone (its ordering and degree
 // class lists), built once on first use and kept with the graph.
 struct GraphCache {
@@ -51,6 +57,7 @@ struct Graph {
     DBuf<i32> col;
     DBuf<W> w;
     DBuf<V> vtx_w;
+    const u64 uid = next_graph_uid();  // identifies the graph to per-context caches
     mutable DBuf<V> rsum;  // row weight sums, computed on first use by the sweep
     std::unique_ptr<GraphCache> cache{new GraphCache()};
     // borrowed (caller-owned) arrays take precedence over the owned ones
@@ -195,7 +202,7 @@ struct MoveStats {
 template <class W>
 void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_part,
                 ClusterState<typename Traits<W>::V>& best, bool is_initial, bool constrained, i32* constraint,
-                bool enable_sa, bool strict, int sweep_limit, MoveStats* stats);
+                bool enable_sa, bool strict, int sweep_limit, MoveStats* stats, bool reuse_pvals = false);
 
 // one select pass (candidates_and_destinations) for parity tests
 template <class W>
@@ -222,7 +229,8 @@ void coarsen_vtx_w(Context& ctx, const Graph<W>& g, const i32* vcmap, Graph<W>& 
 
 template <class W>
 i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* constraint,
-                    const ClusterState<typename Traits<W>::V>& cs, u32 seed_pick, u32 seed_order, i32* vcmap_out);
+                    const ClusterState<typename Traits<W>::V>& cs, u32 seed_pick, u32 seed_order, i32* vcmap_out,
+                    bool reuse_pvals = false);
 
 // ---------------------------------------------------------------------------
 // multilevel drivers (src/clustering_methods.cpp)
@@ -238,8 +246,10 @@ struct RunStats {
 enum Method { METHOD_LOUVAIN = 0, METHOD_LEIDEN = 1, METHOD_LEIDEN_PLUS = 2 };
 
 template <class W>
+// input_is_last: `input` is the output of the context's last local move (on
+// `top`), so its own-cluster weights are still in the context's workspace
 void leiden_part(Context& ctx, const Graph<W>& top, ClusterState<typename Traits<W>::V>& rfd, bool plus, bool improve,
-                 const i32* input, u64 seed, i32* labels_out, RunStats* st);
+                 const i32* input, u64 seed, i32* labels_out, RunStats* st, bool input_is_last = false);
 // the method then ex_iters improvement passes (< 0: while the objective rises)
 template <class W>
 void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Traits<W>::V>& cs, int method, int ex_iters,

@@ -513,7 +513,8 @@ struct RBuf {
 
 template <class W>
 i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32* constraint,
-                    const ClusterState<typename Traits<W>::V>& cs, u32 seed_pick, u32 seed_order, i32* vcmap_out) {
+                    const ClusterState<typename Traits<W>::V>& cs, u32 seed_pick, u32 seed_order, i32* vcmap_out,
+                    bool reuse_pvals) {
     using V = typename Traits<W>::V;
     const i64 n = g.n;
     if (n == 0) return 0;
@@ -528,7 +529,10 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     const int gb = (int)std::min<i64>(std::max<i64>(nmass, 1), (i64)ctx.num_sms * 2);
 
     RBuf<V> pv(ctx, RS_PV, n);
-    own_weights<W>(ctx, g, ord, constraint, pv.p);
+    // constraint = the last local move's output on g: its own-cluster weights
+    // are the context's retained ones
+    if (reuse_pvals && ctx.pv_uid == g.uid && ctx.pv_n == n) copy_d2d(ctx, pv.p, (const V*)ctx.pv_ptr, n);
+    else own_weights<W>(ctx, g, ord, constraint, pv.p);
     RBuf<unsigned char> well(ctx, RS_WELL, n);
     k_well<W><<<grid, 256, 0, ctx.stream>>>(gv, constraint, pv.p, cs.total_deg.p, gamma, well.p);
     PGGC_LAUNCH_CHECK();
@@ -635,8 +639,8 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
 }
 
 template i64 coarsen_leidenR<i32>(Context&, const Graph<i32>&, const Ordering&, const i32*, const ClusterState<i64>&, u32,
-                                  u32, i32*);
+                                  u32, i32*, bool);
 template i64 coarsen_leidenR<float>(Context&, const Graph<float>&, const Ordering&, const i32*,
-                                    const ClusterState<double>&, u32, u32, i32*);
+                                    const ClusterState<double>&, u32, u32, i32*, bool);
 
 }  // namespace pggc

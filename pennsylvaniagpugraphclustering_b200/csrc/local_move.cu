@@ -2075,7 +2075,7 @@ struct Mover {
 template <class W>
 void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_part,
                 ClusterState<typename Traits<W>::V>& best, bool is_initial, bool constrained, i32* constraint,
-                bool enable_sa, bool strict, int sweep_limit, MoveStats* stats) {
+                bool enable_sa, bool strict, int sweep_limit, MoveStats* stats, bool reuse_pvals) {
     using V = typename Traits<W>::V;
     const i64 n = g.n;
     if (n == 0) return;
@@ -2096,9 +2096,15 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
     fill<i32>(ctx, m.dest.p, n, NULL_PART);
     if (!strict) m.filter_init();
     ctx.prof_tag = "init";
+    // the caller's partition is the previous local move's output on this graph:
+    // its own-cluster weights are the ones left in pvals_clone
+    const bool reuse = reuse_pvals && !is_initial && ctx.pv_uid == g.uid && ctx.pv_n == n &&
+                       ctx.pv_ptr == (const void*)m.pvals_clone.p;
+    ctx.pv_uid = 0;
     if (!is_initial) {
         m.cdata_init = true;
-        own_weights_impl<W>(ctx, g, ord, m.part.p, m.pvals.p, 0, nullptr, nullptr, &m.cls);
+        if (reuse) copy_d2d(ctx, m.pvals.p, m.pvals_clone.p, n);
+        else own_weights_impl<W>(ctx, g, ord, m.part.p, m.pvals.p, 0, nullptr, nullptr, &m.cls);
     } else {
         m.cdata_init = false;
         PGGC_CUDA(cudaMemsetAsync(m.pvals.p, 0, sizeof(V) * n, ctx.stream));
@@ -2183,6 +2189,9 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
     ctx.check_device_error();
     m.relabel(best_part, best);
     ctx.prof_tag = nullptr;
+    ctx.pv_uid = g.uid;
+    ctx.pv_ptr = m.pvals_clone.p;
+    ctx.pv_n = n;
     if (stats) {
         stats->sweeps += sweeps;
         stats->moves += total_moves;
@@ -2212,7 +2221,7 @@ i64 select_pass(Context& ctx, const Graph<W>& g, const Ordering& ord, const i32*
 #define PGGC_INST_LM(W)                                                                                             \
     template ClassLists graph_class_lists<W>(Context&, const Graph<W>&, const Ordering&);                           \
     template void local_move<W>(Context&, const Graph<W>&, const Ordering&, i32*, ClusterState<Traits<W>::V>&, bool, \
-                                bool, i32*, bool, bool, int, MoveStats*);                                           \
+                                bool, i32*, bool, bool, int, MoveStats*, bool);                                     \
     template i64 select_pass<W>(Context&, const Graph<W>&, const Ordering&, const i32*, const Traits<W>::V*,         \
                                 ClusterState<Traits<W>::V>&, i32*, float*, float, bool, bool, const i32*);          \
     template void own_weights<W>(Context&, const Graph<W>&, const Ordering&, const i32*, Traits<W>::V*);          \
