@@ -240,8 +240,9 @@ struct Context {
         prof.clear();
     }
 
-    void check_device_error() {
-        int e = read1(d_err);
+    void check_device_error() { raise_device_error(read1(d_err)); }
+    // for a caller that read the error word together with other results
+    void raise_device_error(int e) {
         if (e != DEV_OK) {
             PGGC_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), stream));
             sync();

@@ -809,9 +809,11 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     }
     WsBuf<i64> tstart(ctx, CS_TSTART, nc + 1);
     scan_apply(ctx, ListUIn{ph.p, ucount.p, counts.p + 11}, ArrOutExcl{tstart.p}, nc + 1, nullptr, counts.p + 12);
+    // the device error word rides along in counts[15] (zeroed above)
+    PGGC_CUDA(cudaMemcpyAsync(counts.p + 15, ctx.d_err, sizeof(int), cudaMemcpyDeviceToDevice, ctx.stream));
     const i64* pc = (const i64*)ctx.readback(counts.p, 16 * sizeof(i64));
     const i64 p_w = pc[7], p_r = pc[8], p_b = pc[9], p_b2 = pc[10], p_h = pc[11], nnz_c = pc[14], tn = pc[12];
-    ctx.check_device_error();
+    ctx.raise_device_error((int)pc[15]);
     cg->nnz = nnz_c;
     cg->col = DBuf<i32>(ctx, std::max<i64>(nnz_c, 1));
     cg->w = DBuf<W>(ctx, std::max<i64>(nnz_c, 1));

@@ -624,12 +624,16 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
 
     // --- contigitize
     RBuf<i32> newid(ctx, RS_NEWID, n);
-    RBuf<i64> tot(ctx, RS_TOT, 1);
+    RBuf<i64> tot(ctx, RS_TOT, 2);
     scan_apply(ctx, RootFlag{vcmap.p}, RootEpi{newid.p}, n, nullptr, tot.p);
     k_contig_apply<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, newid.p, vcmap_out);
     PGGC_LAUNCH_CHECK();
-    i64 nc = ctx.read1(tot.p);
-    ctx.check_device_error();
+    // the count and the device error word in one round trip
+    PGGC_CUDA(cudaMemsetAsync(tot.p + 1, 0, sizeof(i64), ctx.stream));
+    PGGC_CUDA(cudaMemcpyAsync(tot.p + 1, ctx.d_err, sizeof(int), cudaMemcpyDeviceToDevice, ctx.stream));
+    const i64* ht = (const i64*)ctx.readback(tot.p, 2 * sizeof(i64));
+    const i64 nc = ht[0];
+    ctx.raise_device_error((int)ht[1]);
     // algorithmic bytes: two adjacency passes (pick, inner connectivity) each
     // reading column, weight, constraint and label of the neighbour; about ten
     // n-sized int32 passes (orderings, sort keys, trees, breaks, relabel)

@@ -33,7 +33,9 @@ struct LMScalars {
     double sumsq_d;
     double obj, best_obj;
     int improved;
-    int pad[3];
+    int err;  // copy of the context's device error word (end of a local move)
+    int pad[2];
+    i64 relabel_count;  // labels after the final relabel
 };
 
 __device__ __forceinline__ void vatomic_add(i64* a, i64 x) { ::atomicAdd((unsigned long long*)a, (unsigned long long)x); }
@@ -1582,8 +1584,13 @@ struct I64ExclOut {
 // ---------------------------------------------------------------------------
 // relabel_contiguously (src/local_mover.cpp:100-129)
 // ---------------------------------------------------------------------------
-__global__ void k_mark_used(unsigned char* used, const i32* lab, i64 n) {
-    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) used[lab[i]] = 1;
+// labels outside [0, L) (only after a device error latched d_err, which the
+// host raises right after) are left alone
+__global__ void k_mark_used(unsigned char* used, const i32* lab, i64 n, i64 L) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        const i32 l = lab[i];
+        if (l >= 0 && l < L) used[l] = 1;
+    }
 }
 struct UsedFlag {
     const unsigned char* used;
@@ -1601,9 +1608,11 @@ struct RelabelEpi {
         }
     }
 };
-__global__ void k_remap(i32* lab, i64 n, const i32* newid) {
-    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
-        lab[i] = newid[lab[i]];
+__global__ void k_remap(i32* lab, i64 n, const i32* newid, i64 L) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        const i32 l = lab[i];
+        if (l >= 0 && l < L) lab[i] = newid[l];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2054,21 +2063,19 @@ struct Mover {
         PGGC_LAUNCH_CHECK();
     }
 
-    void relabel(i32* best_part, ClusterState<V>& best) {
-        i64 L = best.label_count;
+    // relabel_contiguously of the best partition, queued without a host round
+    // trip: L bounds its label count; the new count lands in sc.relabel_count
+    // and the compacted volumes in td2 (copied back by the caller)
+    void relabel_async(i32* best_part, const V* td_best, i64 L, DBuf<V>& td2) {
         DBuf<unsigned char> used(ctx, std::max<i64>(L, 1));
         DBuf<i32> newid(ctx, std::max<i64>(L, 1));
-        DBuf<V> td2(ctx, std::max<i64>(L, 1));
-        DBuf<i64> tot(ctx, 1);
+        td2 = DBuf<V>(ctx, std::max<i64>(L, 1));
         PGGC_CUDA(cudaMemsetAsync(used.p, 0, std::max<i64>(L, 1), ctx.stream));
-        k_mark_used<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(used.p, best_part, n);
+        k_mark_used<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(used.p, best_part, n, L);
         PGGC_LAUNCH_CHECK();
-        scan_apply(ctx, UsedFlag{used.p}, RelabelEpi<V>{newid.p, best.total_deg.p, td2.p}, L, nullptr, tot.p);
-        k_remap<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(best_part, n, newid.p);
+        scan_apply(ctx, UsedFlag{used.p}, RelabelEpi<V>{newid.p, td_best, td2.p}, L, nullptr, &sc.p->relabel_count);
+        k_remap<<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(best_part, n, newid.p, L);
         PGGC_LAUNCH_CHECK();
-        i64 t = ctx.read1(tot.p);
-        copy_d2d(ctx, best.total_deg.p, td2.p, t);
-        best.label_count = t;
     }
 };
 
@@ -2182,12 +2189,17 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
         }
     }
     ctx.prof_tag = "end";
+    // relabel, the device error word and the best state's scalars in one round trip
+    DBuf<V> td2;
+    m.relabel_async(best_part, best.total_deg.p, std::max<i64>(label_bound, best.label_count), td2);
+    PGGC_CUDA(cudaMemcpyAsync(&m.sc.p->err, ctx.d_err, sizeof(int), cudaMemcpyDeviceToDevice, ctx.stream));
     const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
-    best.label_count = hs->best_label_count;
+    const int err = hs->err;
     best.uncut = hs->best_uncut;
     best.obj = hs->best_obj;
-    ctx.check_device_error();
-    m.relabel(best_part, best);
+    best.label_count = hs->relabel_count;
+    ctx.raise_device_error(err);
+    copy_d2d(ctx, best.total_deg.p, td2.p, best.label_count);
     ctx.prof_tag = nullptr;
     ctx.pv_uid = g.uid;
     ctx.pv_ptr = m.pvals_clone.p;
