@@ -344,6 +344,7 @@ def ours(args):
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": int(launches),
+        "ms_each": [round(t, 1) for t in times],
     }
     if bl is not None:
         line["batched_learned"] = bl

@@ -2189,16 +2189,17 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
         }
     }
     ctx.prof_tag = "end";
-    // relabel, the device error word and the best state's scalars in one round trip
-    DBuf<V> td2;
-    m.relabel_async(best_part, best.total_deg.p, std::max<i64>(label_bound, best.label_count), td2);
+    // the best state's scalars and the device error word in one round trip
     PGGC_CUDA(cudaMemcpyAsync(&m.sc.p->err, ctx.d_err, sizeof(int), cudaMemcpyDeviceToDevice, ctx.stream));
     const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
     const int err = hs->err;
+    best.label_count = hs->best_label_count;
     best.uncut = hs->best_uncut;
     best.obj = hs->best_obj;
-    best.label_count = hs->relabel_count;
     ctx.raise_device_error(err);
+    DBuf<V> td2;
+    m.relabel_async(best_part, best.total_deg.p, best.label_count, td2);
+    best.label_count = ctx.read1(&m.sc.p->relabel_count);
     copy_d2d(ctx, best.total_deg.p, td2.p, best.label_count);
     ctx.prof_tag = nullptr;
     ctx.pv_uid = g.uid;
