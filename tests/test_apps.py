@@ -129,3 +129,29 @@ def test_vertex_weights_file_with_lcc(mem, tmp_path):
     cd = pg.get_objective(mem, wg, pg.OBJ_NLCC, 1.0)
     labels, _ = pg.run_clustering(mem, wg, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=3)
     assert np.array_equal(pg.load_view(wg.n, out, np.int32), labels)
+
+
+def test_metrics_records_are_one_json_array(tmp_path):
+    """The -metrics writer (ExperimentLoggerUtil::log format): one object per
+    trial appended to a single JSON array, keys and fixed-point numbers as the
+    reference writes them."""
+    import shutil
+    src = os.path.join(os.path.dirname(os.path.abspath(__file__)), "native", "metrics_log.cpp")
+    exe = tmp_path / "metrics_log"
+    cxx = shutil.which("g++") or "/usr/bin/g++"
+    subprocess.run([cxx, "-std=c++17", "-O1", "-I", B.INCLUDE, "-I", os.path.join(B.HERE, "apps"), src, "-o",
+                    str(exe)], check=True)
+    out = tmp_path / "m.json"
+    subprocess.run([str(exe), str(out)], check=True)
+    text = out.read_text()
+    recs = json.loads(text)
+    assert len(recs) == 3
+    assert recs[0]["edge-cut"] == 1000 and recs[2]["edge-cut"] == 1002.0
+    assert abs(recs[1]["modularity"] - 0.51) < 1e-9
+    assert recs[2]["level-count"] == 6 and recs[0]["total-nnz"] == 123456
+    for name in ("coarsen-contract", "coarsen", "leiden-refine", "free-graph", "total"):
+        assert f"{name}-duration-seconds" in recs[0]
+    assert "iter-times-2" in recs[2] and "iter-obj-2" in recs[2] and "iter-obj-1" not in recs[0]
+    assert recs[1]["number-coarse-levels"] == 0
+    # fixed notation with six decimals, as std::fixed writes them
+    assert '"modularity":0.510000' in text
