@@ -315,3 +315,49 @@ def test_local_move_monotone():
         _, st, _ = O.local_move(og, cd2, part, True, sweep_limit=limit)
         assert st.raw_obj >= last
         last = st.raw_obj
+
+
+def objective_numpy(g, w, vw, labels, objective, mult):
+    """The objectives of interface/cluster_data.hpp:38-181 in closed form:
+    obj = uncut - lambda * sum_c vol(c)^2 with the subclass's lambda and
+    normalisation (Mod/WMod: lambda = mult / g_deg, objective = obj / g_deg;
+    CPM: lambda = mult / 2, objective = obj + lambda * n; NLCC: lambda =
+    mult * g_deg / vol^2, objective = obj / g_deg; LCC: lambda = mult)."""
+    src = np.repeat(np.arange(g.n), np.diff(g.rowptr))
+    ww = np.ones(g.nnz) if w is None else w.astype(np.float64)
+    uncut = ww[labels[src] == labels[g.col]].sum()
+    vol = np.zeros(g.n)
+    np.add.at(vol, labels, vw.astype(np.float64))
+    sq = (vol * vol).sum()
+    g_deg = float(g.nnz) if w is None else ww.sum()
+    if objective in (O.OBJ_MOD, O.OBJ_WMOD):
+        gd = float(g.nnz) if objective == O.OBJ_MOD else vw.astype(np.float64).sum()
+        lam = mult / gd
+        return (uncut - lam * sq) / gd
+    if objective == O.OBJ_CPM:
+        lam = mult * 0.5
+        return uncut - lam * sq + lam * g.n
+    if objective == O.OBJ_NLCC:
+        vt = vw.astype(np.float64).sum()
+        lam = mult * g_deg / (vt * vt)
+        return (uncut - lam * sq) / g_deg
+    return uncut - mult * sq
+
+
+@pytest.mark.parametrize("objective", [O.OBJ_CPM, O.OBJ_NLCC, O.OBJ_LCC])
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("mult", [1.0, 0.3])
+def test_other_objectives_against_closed_form(objective, weighted, mult):
+    """CPM, NLCC and LCC values of the oracle (int32 weights) against the
+    closed forms of the reference's cluster_data subclasses, with the default
+    unit vertex weights and with custom ones."""
+    g = G.small_dcsbm(n=3000)
+    w = np.maximum(np.rint(g.w.astype(np.float64) * 4), 1).astype(np.int32) if weighted else None
+    labels = np.random.default_rng(7).integers(0, 60, g.n).astype(np.int32)
+    uses_w = weighted and objective not in (O.OBJ_CPM,)
+    for vw in (None, np.random.default_rng(3).integers(1, 9, g.n).astype(np.int64)):
+        og = O.Graph(g.rowptr, g.col, w if uses_w else None, vtx_w=vw, objective=objective)
+        q, _ = O.verify_objective(og, labels, objective, mult)
+        vw_eff = np.ones(g.n, np.int64) if vw is None else vw
+        ref = objective_numpy(g, w if uses_w else None, vw_eff, labels, objective, mult)
+        assert abs(q - ref) <= 1e-9 * max(1.0, abs(ref))
