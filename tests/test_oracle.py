@@ -361,3 +361,103 @@ def test_other_objectives_against_closed_form(objective, weighted, mult):
         vw_eff = np.ones(g.n, np.int64) if vw is None else vw
         ref = objective_numpy(g, w if uses_w else None, vw_eff, labels, objective, mult)
         assert abs(q - ref) <= 1e-9 * max(1.0, abs(ref))
+
+
+# ---------------------------------------------------------------------------
+# one whole sweep (select, afterburner, moves, best-state relabel) against a
+# pure-Python transliteration of src/local_mover.cpp:280-433 and :1361-1417
+# ---------------------------------------------------------------------------
+
+
+def xorshift32(x):
+    x &= 0xFFFFFFFF
+    x ^= (x << 13) & 0xFFFFFFFF
+    x ^= x >> 17
+    x ^= (x << 5) & 0xFFFFFFFF
+    return x
+
+
+def as_i32(x):
+    return x - (1 << 32) if x >= (1 << 31) else x
+
+
+def canon_sum_py(terms):
+    """32-lane strided accumulation from 0.0, then the xor butterfly."""
+    v = [0.0] * 32
+    for k, t in enumerate(terms):
+        v[k & 31] = v[k & 31] + t
+    for d in (16, 8, 4, 2, 1):
+        v = [v[l] + v[l ^ d] for l in range(32)]
+    return v[0]
+
+
+def afterburner_py(g, vw, part, dest, gain, lam):
+    eps = f32(0.1)
+    pm = f32(lam)
+    keep = {}
+    for i in range(g.n):
+        best = int(dest[i])
+        if best == O.NO_MOVE:
+            continue
+        p = int(part[i])
+        multi = f32(f32(int(vw[i])) * pm)
+        igain = f32(gain[i])
+        hi = as_i32(xorshift32(i))
+        terms = []
+        for j in range(g.rowptr[i], g.rowptr[i + 1]):
+            v = int(g.col[j])
+            d = f32(f32(gain[v]) - igain)
+            if d >= eps or (abs(d) < eps and as_i32(xorshift32(v)) < hi):
+                q = f32(f32(1.0) - f32(multi * f32(int(vw[v]))))
+                coef = 0
+                if int(dest[v]) == p:
+                    coef -= 1
+                if int(dest[v]) == best and best != O.NEW_PART:
+                    coef += 1
+                if int(part[v]) == p:
+                    coef += 1
+                if int(part[v]) == best:
+                    coef -= 1
+                terms.append(float(coef) * float(q))
+            else:
+                terms.append(0.0)
+        keep[i] = f32(igain + f32(canon_sum_py(terms))) >= 0
+    return keep
+
+
+@pytest.mark.parametrize("graph", ["ring", "sbm"])
+def test_first_sweep_against_python(graph):
+    """Singletons, one annealed sweep (filter ratio 0.75): the oracle's best
+    partition equals the transliteration's moved partition, relabelled in
+    label order, when the sweep raises modularity."""
+    g = G.ring_of_cliques(12, 6) if graph == "ring" else G.from_edges(
+        200, [tuple(e) for e in np.random.default_rng(5).integers(0, 200, (700, 2)) if e[0] != e[1]])
+    if graph == "sbm":  # the edge list may hold duplicates: keep the first of each pair
+        src = np.repeat(np.arange(g.n), np.diff(g.rowptr))
+        keep = np.ones(g.nnz, bool)
+        keep[1:] = (src[1:] != src[:-1]) | (g.col[1:] != g.col[:-1])
+        src, col = src[keep], g.col[keep]
+        rowptr = np.zeros(g.n + 1, np.int64)
+        np.add.at(rowptr, src + 1, 1)
+        g = G.HostGraph(np.cumsum(rowptr), col.astype(np.int32), None, name="random")
+    og = O.Graph(g.rowptr, g.col, objective=O.OBJ_MOD)
+    cd = O.ClusterData(og, O.OBJ_MOD, 1.0)
+    _, _, _, vw = og.arrays()
+    n = g.n
+    lam = cd.info()["lambda"]
+    part = np.arange(n, dtype=np.int32)
+    dest, gain = select_py(g, vw, part, np.zeros(n, np.int64), vw.copy(), lam, 0.75, True,
+                           np.full(n, O.NULL_PART, np.int32))
+    keep = afterburner_py(g, vw, part, dest, gain, lam)
+    moved = part.copy()
+    for i, k in keep.items():
+        if k:
+            moved[i] = dest[i]
+    q_before, _ = O.verify_objective(og, part, O.OBJ_MOD)
+    q_after, _ = O.verify_objective(og, moved, O.OBJ_MOD)
+    out, _, _ = O.local_move(og, cd, part, True, enable_sa=True, sweep_limit=1)
+    if q_after > q_before:
+        _, expect = np.unique(moved, return_inverse=True)
+        assert np.array_equal(out, expect.astype(np.int32))
+    else:
+        assert np.array_equal(out, part)
