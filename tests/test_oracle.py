@@ -461,3 +461,134 @@ def test_first_sweep_against_python(graph):
         assert np.array_equal(out, expect.astype(np.int32))
     else:
         assert np.array_equal(out, part)
+
+
+# ---------------------------------------------------------------------------
+# coarsen_leidenR (src/leidenR.cpp:41-500, unit weights) against a pure-Python
+# transliteration
+# ---------------------------------------------------------------------------
+
+
+def c_mod(a, b):
+    """C's % on signed operands (the remainder takes the dividend's sign)."""
+    r = abs(a) % abs(b)
+    return -r if a < 0 else r
+
+
+def leidenR_py(g, vw, constraint, td, lam, seed_pick, seed_order):
+    n = g.n
+    SPLIT = 1000000000
+    ORD_MAX = 2147483647
+    gamma = f32(lam)
+    src = np.repeat(np.arange(n), np.diff(g.rowptr))
+    pv = np.zeros(n, np.int64)
+    np.add.at(pv, src[constraint[src] == constraint[g.col]], 1)
+    well = [f32(int(pv[i])) >= f32(f32(gamma * f32(int(vw[i]))) * f32(int(td[constraint[i]]) - int(vw[i])))
+            for i in range(n)]
+    hn = list(range(n))
+    for i in range(n):
+        b, e = int(g.rowptr[i]), int(g.rowptr[i + 1])
+        width = e - b
+        multi = f32(gamma * f32(int(vw[i])))
+        jxs = as_i32(murmur3_py((seed_pick + i) & 0xFFFFFFFF))
+        if c_mod(jxs, 1000) == 0 or not well[i] or width == 0:
+            continue
+        jx = b + (jxs & 0xFFFFFFFF) % width
+        for s in range(width):
+            j = jx + s
+            if j >= e:
+                j -= width
+            v = int(g.col[j])
+            if constraint[i] != constraint[v] or not well[v]:
+                continue
+            if f32(1.0) >= f32(multi * f32(int(vw[v]))):
+                hn[i] = v
+                break
+    order = [abs(c_mod(as_i32(murmur3_py((i + seed_order) & 0xFFFFFFFF)), SPLIT)) for i in range(n)]
+    for i in range(n):
+        if order[i] == order[hn[i]]:
+            hn[i] = i
+    vcmap = [ORD_MAX] * n
+    for i in range(n):  # find_trees, src/leidenR.cpp:213-260
+        now, then = i, hn[i]
+        if now == then:
+            vcmap[i] = i
+            continue
+        while order[now] > order[then]:
+            now, then = then, hn[then]
+        if now != i:
+            vcmap[i] = now
+            vcmap[now] = now
+    for i in range(n):
+        if vcmap[i] == ORD_MAX:
+            order[i] = 2 * SPLIT - order[i]
+    unassigned = [vcmap[i] == ORD_MAX for i in range(n)]
+    for i in range(n):
+        if not unassigned[i]:
+            continue
+        now, then = i, hn[i]
+        while vcmap[now] == ORD_MAX and order[now] > order[then]:
+            now, then = then, hn[then]
+        vcmap[i] = vcmap[now]
+    # ensure_gamma_connectivity, src/leidenR.cpp:41-187
+    ids = sorted(range(n), key=lambda a: (vcmap[a], order[a], a))
+    start = {}
+    for x, i in enumerate(ids):
+        start.setdefault(vcmap[i], x)
+    ts, s = [0] * n, 0
+    for x, i in enumerate(ids):
+        ts[x] = s
+        s += int(vw[i])
+    inner = [0] * n
+    for i in range(n):
+        for j in range(g.rowptr[i], g.rowptr[i + 1]):
+            v = int(g.col[j])
+            if vcmap[i] == vcmap[v] and order[v] < order[i]:
+                inner[i] += 1
+    breakers = {}
+    for x, i in enumerate(ids):
+        c = vcmap[i]
+        prev = ts[x] - ts[start[c]]
+        if f32(inner[i]) < f32(f32(gamma * f32(int(vw[i]))) * f32(prev)):
+            breakers[c] = min(breakers.get(c, n), x)
+    oc, s = [0] * n, 0
+    for x, i in enumerate(ids):
+        s += int(pv[i]) - 2 * inner[i]
+        oc[i] = s
+    for x, i in enumerate(ids):
+        c = vcmap[i]
+        cb = start[c]
+        curr = ts[x] + int(vw[i]) - ts[cb]
+        other = int(td[constraint[i]]) - curr
+        outer = oc[i] - (oc[ids[cb - 1]] if cb > 0 else 0)
+        if f32(outer) < f32(f32(gamma * f32(curr)) * f32(other)):
+            breakers[c] = min(breakers.get(c, n), x + 1)
+    for x, i in enumerate(ids):
+        if x >= breakers.get(vcmap[i], n):
+            vcmap[i] = i
+    nc = 0  # contigitize, src/leidenR.cpp:190-210
+    for u in range(n):
+        if vcmap[u] == u:
+            vcmap[u] = nc
+            nc += 1
+        else:
+            vcmap[u] += n
+    for u in range(n):
+        if vcmap[u] >= n:
+            vcmap[u] = vcmap[vcmap[u] - n]
+    return np.array(vcmap, np.int32), nc
+
+
+@pytest.mark.parametrize("seeds", [(1, 2), (12345, 678), (0xDEADBEEF, 0x12345678)])
+def test_leidenR_against_python(seeds):
+    g = G.small_sbm()
+    og = O.Graph(g.rowptr, g.col, objective=O.OBJ_MOD)
+    cd = O.ClusterData(og, O.OBJ_MOD, 1.0)
+    _, _, _, vw = og.arrays()
+    louv, _, _ = O.local_move(og, cd, np.arange(g.n, dtype=np.int32), True)
+    td = cd.total_deg()
+    vo, nco = O.coarsen_leidenR(og, cd, louv, *seeds)
+    vp, ncp = leidenR_py(g, vw, louv, td, cd.info()["lambda"], *seeds)
+    assert nco == ncp
+    assert np.array_equal(vo, vp)
+    assert 0 < nco < g.n
