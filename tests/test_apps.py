@@ -155,3 +155,20 @@ def test_metrics_records_are_one_json_array(tmp_path):
     assert recs[1]["number-coarse-levels"] == 0
     # fixed notation with six decimals, as std::fixed writes them
     assert '"modularity":0.510000' in text
+
+
+def test_option_clamping_printed_before_any_device_work(tmp_path):
+    """parse_args.cpp clamps: -trials below 1 -> 1, -ex_iters below -1 -> -1,
+    -pop_size below 10 -> 10 and -time_limit below 10 -> 10 (with warnings).
+    The configuration is printed before the device is touched, so this runs
+    anywhere (the missing graph file ends the run afterwards)."""
+    missing = tmp_path / "absent.mtx"
+    r = _run("pleiden+", "-i", missing, "-trials", "0", "-ex_iters", "-7")
+    assert r.returncode == 255
+    assert "-- Total trial count: 1" in r.stdout
+    assert "-- Successive Iteration Count: -1" in r.stdout
+    r = _run("meme", "-i", missing, "-pop_size", "3", "-time_limit", "2")
+    assert r.returncode == 255
+    assert "Setting population size to 10." in r.stdout
+    assert "Setting time limit to 10s." in r.stdout
+    assert "-- Population Size: 10" in r.stdout and "-- Time Limit Seconds: 10" in r.stdout
