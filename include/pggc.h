@@ -159,7 +159,14 @@ pggc_status pggc_generate_orderings(pggc_context* ctx, const pggc_graph* g, int3
  * (held by every GPU that loads it until exit), so n is limited to 16,777,216
  * (larger n returns PGGC_ERR_INVALID).  The first call on a device looks up the
  * array's device address; make that first call before any stream capture.
- * All calls share the one array: calls whose work overlaps on the GPU race. */
+ * All calls share the one array: calls whose work overlaps on the GPU race.
+ * Output: the two orderings and the four offsets only (no maximum degree, no
+ * list of the vertices above 4096 edges, which pggc_generate_orderings keeps
+ * with the graph).  Precondition: rowptr is non-decreasing.  The call does not
+ * check it (the offsets live on the device and the call does not wait); a
+ * decreasing pair puts that vertex in the lowest degree bucket, so the outputs
+ * stay permutations of 0..n-1 and no write leaves them, but they are then not
+ * the reference's orderings. */
 pggc_status pggc_generate_orderings_noalloc(const int64_t* rowptr, int64_t n, int32_t* order1, int32_t* order2,
                                             int64_t* offsets, void* stream);
 
@@ -222,7 +229,8 @@ pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_clu
  * pggc_run_clustering calls with the same arguments.  `streams` is an upper
  * bound: one stream per 32 Mi directed edges of the largest graph is used
  * (concurrent runs on graphs that fill the device are slower than sequential
- * ones). */
+ * ones).  Batch calls on one context are serialised: a second call from
+ * another host thread waits until the first has finished. */
 typedef struct pggc_batch_job {
     const pggc_graph* graph;
     int objective;

@@ -22,6 +22,9 @@ struct pggc_context {
     // extra streams for pggc_batch_run, created on first use and kept
     std::mutex workers_mu;
     std::vector<std::unique_ptr<Context>> workers;
+    // held for a whole pggc_batch_run: two batches on one context would
+    // otherwise drive the same worker contexts at once
+    std::mutex batch_mu;
 };
 
 static void ctx_retain(pggc_context* c) { c->refs.fetch_add(1); }
@@ -880,6 +883,7 @@ pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t coun
         }
         need(c.filt.mode != 1, "sample logging is not supported in batched runs");
         if (count == 0) return;
+        std::lock_guard<std::mutex> batch_lock(ctx->batch_mu);
         c.sync();
         // Runs on large graphs already fill the device; concurrent ones then
         // contend for L2 and the launch path and were measured slower than

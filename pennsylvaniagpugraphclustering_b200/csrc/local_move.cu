@@ -1686,6 +1686,7 @@ struct Mover {
     View<i32> gkeys;
     View<V> gvals;
     i64 gcap = 0;
+    int gblocks = 0;  // global tables (one per block of the global-table pass)
     bool cdata_init = false;
     ClassLists cls;
     // learned filter state (allocated only when the context's filter is on)
@@ -1721,9 +1722,14 @@ struct Mover {
         cls = graph_class_lists<W>(ctx, g, ord);
         if (ord.n_huge > 0) {
             gcap = next_pow2_u32((u32)std::min<i64>(2 * ord.max_deg, (i64)1 << 30));
-            i64 nb = std::min<i64>(ord.n_huge, 32);
-            gkeys.p = ctx.ws_get<i32>(S_GK, gcap * nb);
-            gvals.p = ctx.ws_get<V>(S_GV, gcap * nb);
+            // at most 32 tables and at most GTABLE_BYTES of them in total (one
+            // table when a single one is larger): a vertex of degree ~10^7
+            // would otherwise ask for 32 tables of 2^25 slots
+            constexpr i64 GTABLE_BYTES = (i64)1 << 30;
+            const i64 per = gcap * (i64)(sizeof(i32) + sizeof(V));
+            gblocks = (int)std::max<i64>(1, std::min<i64>(std::min<i64>(ord.n_huge, 32), GTABLE_BYTES / per));
+            gkeys.p = ctx.ws_get<i32>(S_GK, gcap * gblocks);
+            gvals.p = ctx.ws_get<V>(S_GV, gcap * gblocks);
         }
     }
 
@@ -1874,8 +1880,7 @@ struct Mover {
             k_select_block<W, CON, false, 1024, true><<<grid, 1024, slot * TS, ctx.stream>>>(
                 ah, host_range(ord.huge.p, 0, ord.n_huge), nullptr, nullptr, TS, ovf, ovf_cnt);
             PGGC_LAUNCH_CHECK();
-            int ggrid = (int)std::min<i64>(ord.n_huge, 32);
-            k_select_block<W, CON, true><<<ggrid, 256, 0, ctx.stream>>>(a, Range{ovf, nullptr, ovf_cnt, 0, 0}, gkeys.p,
+            k_select_block<W, CON, true><<<gblocks, 256, 0, ctx.stream>>>(a, Range{ovf, nullptr, ovf_cnt, 0, 0}, gkeys.p,
                                                                         gvals.p, gcap);
             PGGC_LAUNCH_CHECK();
         }

@@ -15,6 +15,9 @@ namespace pggc {
 
 constexpr int ORD_THREADS = 1024;
 
+// A negative "degree" (a decreasing row-offset pair, which only an invalid
+// CSR has) falls in bucket 0 in both kernels, so the count and scatter passes
+// agree and every write stays inside the two permutations.
 __device__ __forceinline__ int bucket1(i64 d) { return d < LARGE_CUTOFF ? 0 : (d < MASSIVE_CUTOFF ? 1 : 2); }
 __device__ __forceinline__ int bucket2(i64 d) { return d < MID_CUTOFF ? 0 : (d < MASSIVE_CUTOFF ? 1 : 2); }
 
@@ -26,7 +29,7 @@ __global__ void __launch_bounds__(ORD_THREADS) k_order_count(const i64* rowptr, 
     i64 i = (i64)blockIdx.x * ORD_THREADS + threadIdx.x;
     i64 d = -1;
     if (i < n) d = rowptr[i + 1] - rowptr[i];
-    int b1 = d >= 0 ? bucket1(d) : -1, b2 = d >= 0 ? bucket2(d) : -1;
+    int b1 = i < n ? bucket1(d) : -1, b2 = i < n ? bucket2(d) : -1;
     for (int b = 0; b < 3; b++) {
         unsigned m1 = __ballot_sync(FULL, b1 == b);
         unsigned m2 = __ballot_sync(FULL, b2 == b);
@@ -35,9 +38,11 @@ __global__ void __launch_bounds__(ORD_THREADS) k_order_count(const i64* rowptr, 
             atomicAdd(&c[3 + b], __popc(m2));
         }
     }
-    i64 dm = d;
-    for (int o = 16; o >= 1; o >>= 1) dm = max(dm, __shfl_xor_sync(FULL, dm, o));
-    if (lane_id() == 0 && dm > 0) atomicMax(maxdeg, (unsigned long long)dm);
+    if (maxdeg) {
+        i64 dm = d;
+        for (int o = 16; o >= 1; o >>= 1) dm = max(dm, __shfl_xor_sync(FULL, dm, o));
+        if (lane_id() == 0 && dm > 0) atomicMax(maxdeg, (unsigned long long)dm);
+    }
     __syncthreads();
     if (threadIdx.x < 3) {
         cnt1[(i64)threadIdx.x * nblocks + blockIdx.x] = c[threadIdx.x];
@@ -52,7 +57,7 @@ __global__ void __launch_bounds__(ORD_THREADS) k_order_scatter(const i64* rowptr
     int w = threadIdx.x >> 5;
     i64 d = -1;
     if (i < n) d = rowptr[i + 1] - rowptr[i];
-    int b1 = d >= 0 ? bucket1(d) : -1, b2 = d >= 0 ? bucket2(d) : -1;
+    int b1 = i < n ? bucket1(d) : -1, b2 = i < n ? bucket2(d) : -1;
     int r1 = 0, r2 = 0;
     for (int b = 0; b < 3; b++) {
         unsigned m1 = __ballot_sync(FULL, b1 == b);
@@ -134,8 +139,8 @@ void generate_orderings(Context& ctx, const i64* rowptr, i64 n, Ordering& o) {
 // owns every byte of device memory through its own pool and budget), or a
 // real-time loop that must not touch the driver's allocator.  This entry point serves them: the caller
 // passes the inputs and outputs and a stream, and the only scratch (the
-// per-block bucket counts and the max-degree word) lives in a file-scope
-// __device__ array of fixed size.  That array is part of the module image, so
+// per-block bucket counts) lives in a file-scope __device__ array of fixed
+// size.  That array is part of the module image, so
 // every GPU that loads the library holds it until process exit.
 // ===========================================================================
 namespace pggc {
@@ -144,8 +149,9 @@ namespace pggc {
 constexpr i64 NOALLOC_MAX_BLOCKS = 16384;
 constexpr i64 NOALLOC_MAX_N = NOALLOC_MAX_BLOCKS * ORD_THREADS;
 // layout (int64 words): [0, 3B) order1 bucket counts, [3B, 6B) order2 bucket
-// counts (B = NOALLOC_MAX_BLOCKS), then 8 words for the max-degree counter.
-constexpr i64 NOALLOC_WORDS = 6 * NOALLOC_MAX_BLOCKS + 8;
+// counts (B = NOALLOC_MAX_BLOCKS).  k_order_count rewrites the first 3 * nb
+// words of each half on every call, so nothing needs clearing first.
+constexpr i64 NOALLOC_WORDS = 6 * NOALLOC_MAX_BLOCKS;
 static __device__ __align__(256) long long g_noalloc_scratch[NOALLOC_WORDS];
 
 // In-place exclusive scan of k int64 values by one 1024-thread block; writes the
@@ -173,10 +179,6 @@ __global__ void __launch_bounds__(1024) k_noalloc_scan(i64* cnt1, i64* cnt2, i64
         offsets_out[2] = cnt2[nb];      // offset_mid
         offsets_out[3] = cnt1[2 * nb];  // offset_mid2
     }
-}
-
-__global__ void k_noalloc_clear(i64* words, int count) {
-    if (threadIdx.x < count) words[threadIdx.x] = 0;
 }
 
 }  // namespace pggc
@@ -218,17 +220,16 @@ extern "C" pggc_status pggc_generate_orderings_noalloc(const int64_t* rowptr, in
         cudaStream_t s = (cudaStream_t)stream;
         i64* cnt1 = (i64*)scratch;
         i64* cnt2 = cnt1 + 3 * NOALLOC_MAX_BLOCKS;
-        i64* maxw = cnt1 + 6 * NOALLOC_MAX_BLOCKS;
-        k_noalloc_clear<<<1, 32, 0, s>>>(maxw, 8);
-        PGGC_LAUNCH_CHECK();
         if (n == 0) {
             PGGC_CUDA(cudaMemsetAsync(offsets, 0, 4 * sizeof(int64_t), s));
             return PGGC_OK;
         }
         const i64 nb = ceil_div(n, ORD_THREADS);
         // the counts are fully rewritten by k_order_count; the layout uses the
-        // first 3 * nb words of each half, so the bucket-major strides are nb
-        k_order_count<<<(unsigned)nb, ORD_THREADS, 0, s>>>(rowptr, n, nb, cnt1, cnt2, (unsigned long long*)maxw);
+        // first 3 * nb words of each half, so the bucket-major strides are nb.
+        // No max-degree word: this entry point returns the orderings and the
+        // four bucket offsets only.
+        k_order_count<<<(unsigned)nb, ORD_THREADS, 0, s>>>(rowptr, n, nb, cnt1, cnt2, nullptr);
         PGGC_LAUNCH_CHECK();
         k_noalloc_scan<<<1, 1024, 0, s>>>(cnt1, cnt2, nb, offsets);
         PGGC_LAUNCH_CHECK();

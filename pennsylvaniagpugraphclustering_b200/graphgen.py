@@ -107,10 +107,18 @@ def planted_sbm_65k(seed: int = 1) -> HostGraph:
     return sbm(65536, 64, 16.0, 4.0, seed)
 
 
+# Expected degree before deduplication that leaves a mean degree of 20 after
+# it on the 4,194,304-vertex DC-SBM: pairs drawn twice inside small
+# communities merge, so mean 20 would give 39.06 M edges instead of 41.9 M
+# (seed 1: 41,931,980 undirected edges, mean degree 19.995).
+DCSBM_4M_MEAN_DEG = 21.53
+
+
 def dcsbm_4m(seed: int = 1, n: int = 4194304) -> HostGraph:
-    """pLeiden+ workload: DC-SBM n=4,194,304, degree exp 2.5 (min 5, mean 20), community exp 1.5
-    on [50, 5000], mu=0.4, FP32 weights uniform in [0.5, 1.5)."""
-    return dcsbm(n, seed)
+    """pLeiden+ workload: DC-SBM n=4,194,304, degree exp 2.5 (min 5, mean 20 after deduplication,
+    ~41.9 M undirected edges), community exp 1.5 on [50, 5000], mu=0.4, FP32 weights uniform in
+    [0.5, 1.5)."""
+    return dcsbm(n, seed, mean_deg=DCSBM_4M_MEAN_DEG)
 
 
 def rmat24(seed: int = 1, scale: int = 24) -> HostGraph:
