@@ -63,7 +63,16 @@ typedef struct pggc_stats {
     double objective;    /* cluster_data::get_objective() after the call                      */
     double raw_obj;      /* cluster_data::obj                                                 */
     int64_t label_count; /* cluster_data::label_count                                         */
+    /* learned move filter judge (run_clustering with a filter enabled; 0 otherwise) */
+    int64_t filtered_passes; /* passes run with the filter                                    */
+    int64_t exact_passes;    /* exact (unfiltered) passes the judge ran after them              */
+    double judge_gain;       /* objective change of those exact passes                         */
+    int64_t fell_back;       /* 1 when judge_gain > PGGC_FILTER_TOLERANCE                      */
 } pggc_stats;
+
+/* Modularity the learned filter may give up before its judge counts a fallback
+ * to the plain sweep. */
+#define PGGC_FILTER_TOLERANCE 0.001
 
 const char* pggc_last_error(void);
 /* build-time identification, e.g. "pggc-b200 sm_100a" */

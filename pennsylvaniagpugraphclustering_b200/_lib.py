@@ -36,7 +36,9 @@ class DeviceError(PggcError):
 class Stats(ctypes.Structure):
     _fields_ = [("levels", ctypes.c_int64), ("total_nnz", ctypes.c_int64), ("sweeps", ctypes.c_int64),
                 ("moves", ctypes.c_int64), ("passes", ctypes.c_int64), ("objective", ctypes.c_double),
-                ("raw_obj", ctypes.c_double), ("label_count", ctypes.c_int64)]
+                ("raw_obj", ctypes.c_double), ("label_count", ctypes.c_int64),
+                ("filtered_passes", ctypes.c_int64), ("exact_passes", ctypes.c_int64),
+                ("judge_gain", ctypes.c_double), ("fell_back", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -258,6 +258,10 @@ void fill_stats(pggc_stats* st, const RunStats& rs, double objective, double raw
     st->objective = objective;
     st->raw_obj = raw;
     st->label_count = L;
+    st->filtered_passes = rs.filtered_passes;
+    st->exact_passes = rs.exact_passes;
+    st->judge_gain = rs.judge_gain;
+    st->fell_back = rs.fell_back;
 }
 
 // verify_objective kernels

@@ -75,16 +75,26 @@ struct Context {
         i32 stamp = 0;                          // sweep counter (moved-last-sweep feature)
     } filt;
 
+    // The context's own stream-ordered memory pool.  One pool per context (not
+    // the device's default pool) keeps contexts that run concurrently -- the
+    // workers of a batch -- independent: memory freed on one stream is never
+    // handed to another stream with a dependency on the first one's work.
+    cudaMemPool_t pool = nullptr;
+
     explicit Context(int dev) : device(dev) {
         PGGC_CUDA(cudaSetDevice(dev));
         PGGC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-        cudaMemPool_t pool;
-        PGGC_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        PGGC_CUDA(cudaMemPoolCreate(&pool, &props));
         u64 thr = ~0ull;
         PGGC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-        PGGC_CUDA(cudaMallocAsync((void**)&d_err, sizeof(int) * 8, stream));
+        PGGC_CUDA(dev_malloc((void**)&d_err, sizeof(int) * 8));
         PGGC_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int) * 8, stream));
-        PGGC_CUDA(cudaMallocAsync((void**)&d_prof, sizeof(unsigned long long) * 64, stream));
+        PGGC_CUDA(dev_malloc((void**)&d_prof, sizeof(unsigned long long) * 64));
         PGGC_CUDA(cudaMemsetAsync(d_prof, 0, sizeof(unsigned long long) * 64, stream));
         h_pin_bytes = 4096;
         PGGC_CUDA(cudaMallocHost(&h_pin, h_pin_bytes));
@@ -94,6 +104,8 @@ struct Context {
         max_smem_optin = prop.sharedMemPerBlockOptin;
         PGGC_CUDA(cudaStreamSynchronize(stream));
     }
+    // stream-ordered allocation from the context's pool
+    cudaError_t dev_malloc(void** p, size_t bytes) { return cudaMallocFromPoolAsync(p, bytes, pool, stream); }
     // Stack arena for short-lived temporaries (scan tile sums, reduction
     // partials, sort histograms): LIFO reuse of one device buffer.  Work on the
     // context is ordered on one stream, so a region may be handed out again
@@ -110,7 +122,7 @@ struct Context {
         if (e.second < bytes) {
             if (e.first) PGGC_CUDA(cudaFreeAsync(e.first, stream));
             size_t nb = bytes + bytes / 4;
-            PGGC_CUDA(cudaMallocAsync(&e.first, nb, stream));
+            PGGC_CUDA(dev_malloc(&e.first, nb));
             e.second = nb;
         }
         return (T*)e.first;
@@ -134,6 +146,8 @@ struct Context {
         if (stream) cudaStreamSynchronize(stream);
         if (h_pin) cudaFreeHost(h_pin);
         if (stream) cudaStreamDestroy(stream);
+        // blocks still held by other objects are released when they are freed
+        if (pool) cudaMemPoolDestroy(pool);
     }
     Context(const Context&) = delete;
     Context& operator=(const Context&) = delete;
@@ -145,13 +159,13 @@ struct Context {
         if (profiling) {
             // host time spent in the stream-ordered allocator (pool growth shows here)
             auto t0 = std::chrono::steady_clock::now();
-            PGGC_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (size_t)count, stream));
+            PGGC_CUDA(dev_malloc((void**)&p, sizeof(T) * (size_t)count));
             auto& st = prof["host_alloc"];
             st.launches++;
             st.bytes += (double)(sizeof(T) * (size_t)count);
             st.ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         } else {
-            PGGC_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (size_t)count, stream));
+            PGGC_CUDA(dev_malloc((void**)&p, sizeof(T) * (size_t)count));
         }
         return p;
     }
@@ -302,7 +316,7 @@ struct Tmp {
         if (ctx.arena_top == 0 && ctx.arena_cap < bytes) {
             if (ctx.arena) PGGC_CUDA(cudaFreeAsync(ctx.arena, ctx.stream));
             ctx.arena_cap = std::max<size_t>(bytes, (size_t)64 << 20);
-            PGGC_CUDA(cudaMallocAsync((void**)&ctx.arena, ctx.arena_cap, ctx.stream));
+            PGGC_CUDA(ctx.dev_malloc((void**)&ctx.arena, ctx.arena_cap));
         }
         if (ctx.arena_top + bytes <= ctx.arena_cap) {
             mark = ctx.arena_top;

@@ -16,6 +16,9 @@ namespace pggc {
 // others use shared-memory tables.
 constexpr i64 HUGE_DEG = 4096;
 constexpr int SEL_TS_MAX = 8192;  // shared-memory table slots of the block kernels
+// objective (modularity) the learned move filter may give up before its judge
+// reports a fallback to the plain sweep (PGGC_FILTER_TOLERANCE)
+constexpr double FILTER_TOLERANCE = 0.001;
 
 // ---------------------------------------------------------------------------
 // src/ordering.cpp:131-164 -- stable degree-bucket orderings
@@ -241,6 +244,11 @@ struct RunStats {
     i64 sweeps = 0;
     i64 moves = 0;
     i64 passes = 0;
+    // learned move filter judge (run_clustering with the filter on)
+    i64 filtered_passes = 0;  // passes run with the filter
+    i64 exact_passes = 0;     // exact passes the judge ran after them
+    double judge_gain = 0;    // objective change those exact passes made
+    i64 fell_back = 0;        // 1: the gain exceeded the filter's tolerance
 };
 
 enum Method { METHOD_LOUVAIN = 0, METHOD_LEIDEN = 1, METHOD_LEIDEN_PLUS = 2 };

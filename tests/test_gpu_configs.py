@@ -63,10 +63,15 @@ def test_planted_sbm_65k_plouvain(mem, ex_iters):
     assert so.objective == sg["objective"]
     assert so.label_count == sg["label_count"]
     assert so.levels == sg["levels"]
-    # the planted 64 blocks are found
+    # the planted 64 blocks are found: 64 clusters, each block's majority
+    # label distinct and covering at least 99 % of the block
     assert sg["label_count"] == 64
-    blocks = np.arange(hg.n) // 1024
-    assert len(set(zip(blocks.tolist(), lg.tolist()))) == 64
+    maj = []
+    for b in range(64):
+        cnt = np.bincount(lg[b * 1024:(b + 1) * 1024])
+        maj.append(int(cnt.argmax()))
+        assert cnt.max() >= 0.99 * 1024
+    assert len(set(maj)) == 64
     assert abs(q - sg["objective"]) < 1e-9
 
 
