@@ -1,25 +1,40 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 clustering hot path: pLeiden+ edges/s.
+"""Benchmark of the B200 clustering hot path: Leiden edges/s, batched+learned vs plain.
 
 Workload: pLeiden+ (leiden_part<plus=true> then improvement passes until the
 objective stops rising, i.e. ``-ex_iters -1``) with the weighted-modularity
 objective on a seeded degree-corrected SBM: n = 4,194,304, power-law degrees
 (exponent 2.5, min 5, mean 20), power-law community sizes (exponent 1.5, 50 to
-5,000), mu = 0.4, FP32 edge weights uniform in [0.5, 1.5).  Synthetic data
-stand in for the reference's external graph collection.
+5,000), mu = 0.4, ~41.9 M undirected edges, FP32 edge weights uniform in
+[0.5, 1.5).  Synthetic data stand in for the reference's external graph
+collection.
 
 One step = one full clustering run (run_clustering in app/cluster_main.cpp:116)
-from a fresh cluster_data on the graph already resident in HBM.  The metric is
-undirected input edges / clustering time (the reference's "Cluster time"
-span).  ``e2e`` repeats the step through the public C ABI from host buffers:
-CSR upload, graph + objective construction, clustering and label download.
+of one member of a population of seeds, from a fresh cluster_data on the graph
+already resident in HBM.  The metric is undirected input edges / clustering
+time (the reference's "Cluster time" span), at equal modularity:
+
+* ``value``: the K timed steps run as ONE batch (``pggc_batch_run``, P worker
+  streams) with the learned move filter on, its judge included -- the
+  batched+learned configuration.  Time = CUDA events on the context stream,
+  which the batch's workers are ordered against.
+* ``plain``: R of the same seeds run one after another, no filter, one stream;
+  ``ratio_vs_plain`` = value / plain edges/s, with both modularities (mean over
+  those seeds) and the criterion "ratio >= 1.5 at modularity within 0.001".
+* ``e2e``: a batch of P members through the public C ABI from host buffers:
+  CSR upload, graph + objective construction, clustering and label download.
+
+The filter is trained before the warm-up (untimed) on move labels logged from
+plain first passes of the three named workloads' generators at seeds 1-8:
+planted SBM n = 65,536, the DC-SBM at n = 262,144, R-MAT scale 18.
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (the reference itself needs Kokkos, which is unavailable) on a bounded sample of
-the same workload with all host threads.
+the same workload (a 262,144-vertex DC-SBM with the same parameters) with all
+host threads; our line reports the GPU on that same sample beside it.
 
 Multi-GPU (torchrun): the path does not shard; every rank clusters its own
-replica and ``value`` is the edges of all replicas over the slowest rank's time.
+population and ``value`` is the edges of all ranks over the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -39,8 +54,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Leiden edges/s at equal modularity: batched+learned vs plain, same B200"
 UNIT = "edges/s"
-WORKLOAD = ("pLeiden+ until stable (ex_iters=-1), WMod, DC-SBM n=4,194,304, deg exp 2.5 min 5 mean 20, "
-            "communities exp 1.5 on [50,5000], mu=0.4, FP32 weights U[0.5,1.5), int64 offsets")
+WORKLOAD = ("pLeiden+ until stable (ex_iters=-1), WMod, DC-SBM n=4,194,304, deg exp 2.5 min 5 mean 20 "
+            "(~41.9M undirected edges), communities exp 1.5 on [50,5000], mu=0.4, FP32 weights U[0.5,1.5), "
+            "int64 offsets; population of seeds run as one batch with the learned move filter")
+TARGET_RATIO = 1.5
+Q_TOLERANCE = 0.001
 DOMINANT_FAMILIES = ("select_warp", "select_block", "select_huge", "afterburner_warp", "own_weights", "contract",
                      "leiden_refine", "filter")
 # sub-phases reported beside the families (not candidates for the roofline line)
@@ -50,19 +68,20 @@ SUB_PHASES = ("contract_prep", "contract_hash", "contract_place", "contract_plac
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=8, help="timed clustering runs (population members)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4194304, help="DC-SBM vertex count (default: the named workload)")
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--streams", type=int, default=4, help="worker streams of the batch (population width)")
+    ap.add_argument("--plain-runs", type=int, default=2,
+                    help="plain runs (the first seeds of the population, no filter, one stream) for the ratio")
+    ap.add_argument("--no-filter", action="store_true", help="batched plain runs (no learned filter)")
+    ap.add_argument("--recall", type=float, default=0.98,
+                    help="recall on the training logs that sets the filter's logit threshold")
     ap.add_argument("--cpu-sample-n", type=int, default=262144)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=None)
-    ap.add_argument("--batched-learned", type=int, default=0, metavar="K",
-                    help="also time a population of K seeds run concurrently (pggc_batch_run) with the learned "
-                         "move filter, trained first on logs of plain runs of smaller graphs")
-    ap.add_argument("--recall", type=float, default=0.98,
-                    help="--batched-learned: recall on the training logs that sets the filter threshold")
+    ap.add_argument("--e2e-steps", type=int, default=None, help="e2e batch size (default: --streams)")
     ap.add_argument("--by-level", action="store_true",
                     help="profiled run also splits each kernel family by multilevel level (adds 'by_level')")
     ap.add_argument("--ex-iters", type=int, default=-1,
@@ -136,7 +155,7 @@ class ClockSampler:
 def cpu_run(sample_n: int, seed: int, steps: int, warmup: int):
     from oracle import oracle as O
     from pennsylvaniagpugraphclustering_b200 import graphgen as gg
-    g = gg.dcsbm(sample_n, seed)
+    g = gg.dcsbm(sample_n, seed, mean_deg=gg.DCSBM_4M_MEAN_DEG)
     og = O.Graph(g.rowptr, g.col, g.w, objective=O.OBJ_WMOD)
     times = []
     q = None
@@ -151,6 +170,7 @@ def cpu_run(sample_n: int, seed: int, steps: int, warmup: int):
     sec = statistics.mean(times)
     return {"value": g.m / sec, "unit": UNIT, "cores": int(O.lib().orc_num_threads()), "kind": "port",
             "ms_per_run": sec * 1000.0,
+            "modularity": q, "n": sample_n, "m": g.m,
             "sample": f"DC-SBM n={sample_n} (m={g.m}) with the workload's parameters, seed {seed}; "
                       f"pLeiden+ until stable; {steps} timed runs, mean {sec:.3f} s; modularity {q:.6f}"}
 
@@ -163,7 +183,9 @@ def reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_run"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_n": args.cpu_sample_n},
+            "config": {"workload": WORKLOAD, "sample_n": args.cpu_sample_n, "sample_m": res.get("m"),
+                       "reference_runs": "plain pLeiden+ until stable (the reference has no batching and no "
+                                         "learned filter) on the sample graph, seed " + str(args.seed)},
             "cpu_baseline": res,
             "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "CPU restatement of the reference algorithm (oracle port); the reference needs Kokkos, "
@@ -192,10 +214,50 @@ def traffic_for(family):
         return None
 
 
+
+
+def train_filter(pg, mem, recall):
+    """Train the learned move filter on move labels logged from plain first
+    passes of the named workloads' generators at seeds 1-8 (planted SBM
+    n = 65,536; the DC-SBM at n = 262,144; R-MAT scale 18); returns
+    (params, threshold, info)."""
+    from pennsylvaniagpugraphclustering_b200 import graphgen as gg, move_filter as MF
+    t0 = time.perf_counter()
+    xs, ys = [], []
+    cap = 400_000
+    for s in range(1, 9):
+        for kind in ("sbm", "dcsbm", "rmat"):
+            if kind == "sbm":
+                h, obj, w = gg.planted_sbm_65k(s), pg.OBJ_MOD, None
+            elif kind == "dcsbm":
+                h = gg.dcsbm(262144, s, mean_deg=gg.DCSBM_4M_MEAN_DEG)
+                obj, w = pg.OBJ_WMOD, h.w
+            else:
+                h, obj, w = gg.rmat(18, 16, 0.57, 0.19, 0.19, s), pg.OBJ_MOD, None
+            g2 = pg.weighted_graph(mem, h.rowptr, h.col, w, objective=obj)
+            MF.log_start(mem, capacity=cap, sample_rate=0.1, seed=s)
+            cd = pg.get_objective(mem, g2, obj, 1.0)
+            method = pg.METHOD_LOUVAIN if kind != "dcsbm" else pg.METHOD_LEIDEN_PLUS
+            pg.run_clustering(mem, g2, cd, method=method, ex_iters=0, seed=s)
+            x, y, _ = MF.log_stop(mem, cap)
+            xs.append(x)
+            ys.append(y)
+            cd.close()
+            g2.close()
+    x = np.concatenate(xs)
+    y = np.concatenate(ys)
+    pos_w = float(min(20.0, (len(y) - y.sum()) / max(y.sum(), 1.0)))
+    params, losses = MF.train(mem, MF.init_params(1), x, y, epochs=6, batch=4096, lr=3e-3, pos_weight=pos_w)
+    thr = MF.threshold_for_recall(mem, params, x, y, recall=recall)
+    return params, thr, {"train_rows": int(len(y)), "positive_rows": int(y.sum()), "final_loss": float(losses[-1]),
+                         "threshold_logit": thr, "recall": recall, "train_seconds": time.perf_counter() - t0,
+                         "sources": "first passes of planted SBM 65,536, DC-SBM 262,144 and R-MAT 18, seeds 1-8"}
+
+
 def ours(args):
     import torch
     import pennsylvaniagpugraphclustering_b200 as pg
-    from pennsylvaniagpugraphclustering_b200 import _lib, graphgen as gg
+    from pennsylvaniagpugraphclustering_b200 import _lib, graphgen as gg, move_filter as MF
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -203,25 +265,43 @@ def ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    g = gg.dcsbm(args.n, args.seed)
+    g = gg.dcsbm(args.n, args.seed, mean_deg=gg.DCSBM_4M_MEAN_DEG)
     m = g.m
     mem = pg.memory_store(local)
     stream = torch.cuda.ExternalStream(mem.stream(), device=torch.device("cuda", local))
     wg = pg.weighted_graph(mem, g.rowptr, g.col, g.w, objective=pg.OBJ_WMOD)
-    labels = torch.empty(g.n, dtype=torch.int32, device=f"cuda:{local}")
+    lib = _lib.lib()
+    learned = not args.no_filter
+    K = max(1, args.steps)
+    P = max(1, min(args.streams, K))
+    seeds = [args.seed + rank * 1000 + j for j in range(K)]
 
-    def step(seed):
-        cd = pg.get_objective(mem, wg, pg.OBJ_WMOD, 1.0)
+    filt_info = None
+    params = thr = None
+    if learned:
+        params, thr, filt_info = train_filter(pg, mem, args.recall)
+
+    def jobs(sds, ex=args.ex_iters):
+        return [dict(graph=wg, objective=pg.OBJ_WMOD, method=pg.METHOD_LEIDEN_PLUS, ex_iters=ex, seed=sd)
+                for sd in sds]
+
+    def timed(fn):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        _, st = pg.run_clustering(mem, wg, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=args.ex_iters, seed=seed,
-                                  out=labels)
+        out = fn()
         e1.record(stream)
         e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        cd.close()
-        return ms, st
+        return e0.elapsed_time(e1), out
+
+    def batch(sds, streams):
+        if learned:
+            MF.enable(mem, params, thr)
+        try:
+            return pg.batch_run(mem, jobs(sds), streams=streams)
+        finally:
+            if learned:
+                MF.disable(mem)
 
     def barrier():
         if world > 1:
@@ -229,25 +309,49 @@ def ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    for w in range(args.warmup):
-        step(args.seed + rank)
-    lib = _lib.lib()
+    # warm-up: W runs through the batch path (worker streams, pools, scratch)
+    if args.warmup > 0:
+        batch([args.seed + 500 + j for j in range(args.warmup)], min(P, args.warmup))
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
     l0 = lib.pggc_launch_count()
-    times, stats = [], None
-    for s in range(args.steps):
-        ms, stats = step(args.seed + rank)
-        times.append(ms)
+    if learned:
+        MF.stats(mem, reset=True)
+    ms_batch, res = timed(lambda: batch(seeds, P))
     launches = lib.pggc_launch_count() - l0
     barrier()
     clk = clocks.stop()
-    # one more, untimed run with per-family CUDA events and device byte
-    # counters on: the kernel breakdown and the roofline figures
+    ev, sk = MF.stats(mem) if learned else (0, 0)
+    q_batch = [st["objective"] for _, st in res]
+
+    # plain: the first R seeds, no filter, one after another on one stream
+    R = max(0, min(args.plain_runs, K))
+    plain_ms, plain_q, plain_passes = [], [], []
+    for sd in seeds[:R]:
+        cd = pg.get_objective(mem, wg, pg.OBJ_WMOD, 1.0)
+        ms, (_, st) = timed(lambda: pg.run_clustering(mem, wg, cd, method=pg.METHOD_LEIDEN_PLUS,
+                                                        ex_iters=args.ex_iters, seed=sd))
+        plain_ms.append(ms)
+        plain_q.append(st["objective"])
+        plain_passes.append(st["passes"])
+        cd.close()
+
+    # one more learned run on the context stream with per-family CUDA events
+    # and device byte counters: the kernel breakdown and the roofline figures
     _lib.check(lib.pggc_profile_reset(mem.handle))
     _lib.check(lib.pggc_profile_enable(mem.handle, 2 if args.by_level else 1))
-    step(args.seed + rank)
+    labels = torch.empty(g.n, dtype=torch.int32, device=f"cuda:{local}")
+    if learned:
+        MF.enable(mem, params, thr)
+    try:
+        cd = pg.get_objective(mem, wg, pg.OBJ_WMOD, 1.0)
+        pg.run_clustering(mem, wg, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=args.ex_iters, seed=seeds[0],
+                          out=labels)
+        cd.close()
+    finally:
+        if learned:
+            MF.disable(mem)
     _lib.check(lib.pggc_profile_enable(mem.handle, 0))
     fam = {}
 
@@ -271,39 +375,44 @@ def ours(args):
                 f, lv = name.split("@", 1)
                 n_l, t_ms, _ = read_family(name)
                 by_level.setdefault(f, {})[lv] = {"launches": n_l, "ms": round(t_ms, 3)}
-    q_labels = labels.cpu().numpy()
-    q, _ = pg.verify_objective(mem, wg, q_labels, pg.OBJ_WMOD)
+    q_verify, _ = pg.verify_objective(mem, wg, labels.cpu().numpy(), pg.OBJ_WMOD)
 
-    # e2e: host buffers through the public API, copies inside the timed region
-    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 2))
-    e2e_steps = max(0, e2e_steps)
-    e2e_ms = []
-    host_labels = np.empty(g.n, np.int32)
-    for s in range(e2e_steps):
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        g2 = pg.weighted_graph(mem, g.rowptr, g.col, g.w, objective=pg.OBJ_WMOD)
-        cd2 = pg.get_objective(mem, g2, pg.OBJ_WMOD, 1.0)
-        pg.run_clustering(mem, g2, cd2, method=pg.METHOD_LEIDEN_PLUS, ex_iters=args.ex_iters,
-                          seed=args.seed + rank, out=host_labels)
-        e1.record(stream)
-        e1.synchronize()
-        e2e_ms.append(e0.elapsed_time(e1))
-        cd2.close()
-        g2.close()
+    # e2e: host buffers through the public API (CSR upload, graph and objective
+    # construction, a batch of E members, label download) inside the timed region
+    E = args.e2e_steps if args.e2e_steps is not None else P
+    E = max(0, E)
+    e2e_ms = float("nan")
+    if E > 0:
+        def e2e_once():
+            g2 = pg.weighted_graph(mem, g.rowptr, g.col, g.w, objective=pg.OBJ_WMOD)
+            if learned:
+                MF.enable(mem, params, thr)
+            try:
+                out = pg.batch_run(mem, [dict(graph=g2, objective=pg.OBJ_WMOD, method=pg.METHOD_LEIDEN_PLUS,
+                                              ex_iters=args.ex_iters, seed=sd) for sd in seeds[:E]],
+                                   streams=min(P, E))
+            finally:
+                if learned:
+                    MF.disable(mem)
+            g2.close()
+            return out
+        e2e_ms, _ = timed(e2e_once)
     h2d = g.rowptr.nbytes + g.col.nbytes + g.w.nbytes
-    d2h = host_labels.nbytes
+    d2h = 4 * g.n * E
 
-    ms_step = statistics.mean(times)
-    ms_e2e = statistics.mean(e2e_ms) if e2e_ms else float("nan")
+    ms_step = ms_batch / K
+    ms_plain = statistics.mean(plain_ms) if plain_ms else float("nan")
     if world > 1:
         from pennsylvaniagpugraphclustering_b200 import replicas
-        ms_step, ms_e2e = replicas.max_over_ranks([ms_step, ms_e2e], device=f"cuda:{local}")
+        ms_step, ms_e2e_run, ms_plain = replicas.max_over_ranks([ms_step, e2e_ms / max(E, 1), ms_plain],
+                                                                device=f"cuda:{local}")
+    else:
+        ms_e2e_run = e2e_ms / max(E, 1)
     value = world * m / (ms_step / 1000.0)
-    e2e_value = world * m / (ms_e2e / 1000.0)
+    e2e_value = world * m / (ms_e2e_run / 1000.0)
+    plain_value = world * m / (ms_plain / 1000.0) if plain_ms else None
 
-    # roofline for the dominant instrumented kernel
+    # roofline for the dominant instrumented kernel family
     dom = max((f for f in DOMINANT_FAMILIES if fam[f][2] > 0), key=lambda f: fam[f][1], default=None)
     peak, peak_kind = peaks()
     roof = None
@@ -320,34 +429,67 @@ def ours(args):
             import torch.distributed as dist
             dist.destroy_process_group()
         return
-    bl = None
-    if args.batched_learned > 0:
-        bl = batched_learned(args, pg, mem, wg, m, q)
     cpu = None
+    same_sample = None
     if world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_run(args.cpu_sample_n, args.seed, 1, 0)
+            # the GPU on the same sample graph and seed: like-for-like speed,
+            # identical modularity (the two paths share one arithmetic)
+            h = gg.dcsbm(args.cpu_sample_n, args.seed, mean_deg=gg.DCSBM_4M_MEAN_DEG)
+            g3 = pg.weighted_graph(mem, h.rowptr, h.col, h.w, objective=pg.OBJ_WMOD)
+            t3 = []
+            for _ in range(3):
+                cd = pg.get_objective(mem, g3, pg.OBJ_WMOD, 1.0)
+                ms3, (_, st3) = timed(lambda: pg.run_clustering(mem, g3, cd, method=pg.METHOD_LEIDEN_PLUS,
+                                                                  ex_iters=-1, seed=args.seed))
+                t3.append(ms3)
+                cd.close()
+            g3.close()
+            gpu_v = h.m / (min(t3) / 1000.0)
+            same_sample = {"n": args.cpu_sample_n, "m": h.m, "gpu_plain_edges_per_s": gpu_v,
+                           "cpu_edges_per_s": cpu["value"], "gpu_over_cpu": gpu_v / cpu["value"],
+                           "gpu_modularity": st3["objective"], "cpu_modularity": cpu["modularity"],
+                           "identical_modularity": st3["objective"] == cpu["modularity"]}
         except Exception as ex:  # report, never fail the line
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+    q_mean = statistics.mean(q_batch[:R]) if R else statistics.mean(q_batch)
+    plain_q_mean = statistics.mean(plain_q) if plain_q else None
+    dq = (q_mean - plain_q_mean) if plain_q_mean is not None else None
+    ratio = value / plain_value if plain_value else None
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded DC-SBM)",
-        "config": {"workload": WORKLOAD, "n": g.n, "m_undirected": m, "nnz": g.nnz, "seed": args.seed,
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (graph CSR ~0.7 GB)",
-                   "modularity": q, "levels": stats["levels"], "passes": stats["passes"],
-                   "sweeps": stats["sweeps"], "labels": stats["label_count"]},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "ms_per_step": ms_e2e, "ms_each": e2e_ms},
+        "config": {"workload": WORKLOAD, "n": g.n, "m_undirected": m, "nnz": g.nnz, "seeds": [seeds[0], seeds[-1]],
+                   "parallelism": f"replicas x{world}; batch of {K} runs on {P} streams per GPU",
+                   "learned_filter": learned, "l2": "inputs larger than L2 (graph CSR ~0.7 GB)",
+                   "modularity_mean": statistics.mean(q_batch), "modularity_min": min(q_batch),
+                   "passes_mean": statistics.mean(st["passes"] for _, st in res),
+                   "exact_passes_mean": statistics.mean(st["exact_passes"] for _, st in res),
+                   "fallbacks": int(sum(st["fell_back"] for _, st in res)),
+                   "sweeps_mean": statistics.mean(st["sweeps"] for _, st in res),
+                   "labels_mean": statistics.mean(st["label_count"] for _, st in res),
+                   "filter_skipped_frac": sk / max(ev + sk, 1) if learned else 0.0},
+        "plain": {"value": plain_value, "unit": UNIT, "runs": R, "ms_per_run": ms_plain,
+                  "modularity_mean": plain_q_mean, "passes_mean": statistics.mean(plain_passes) if R else None,
+                  "seeds": seeds[:R]},
+        "ratio_vs_plain": ratio,
+        "modularity_delta_vs_plain": dq,
+        "criterion": {"ratio_min": TARGET_RATIO, "modularity_tolerance": Q_TOLERANCE,
+                      "met": bool(ratio is not None and ratio >= TARGET_RATIO and dq is not None and dq >= -Q_TOLERANCE)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d / max(E, 1)),
+                "d2h_bytes_per_step": int(d2h / max(E, 1)), "ms_per_step": ms_e2e_run, "batch": E,
+                "note": "CSR uploaded once per batch of E runs (bytes per step = upload / E)"},
         "roofline": roof,
         "kernel_families": {f: {"launches": v[0], "ms": v[1], "alg_bytes": v[2]} for f, v in fam.items()},
+        "profiled_run_verify_modularity": q_verify,
         "cpu_baseline": cpu,
+        "same_sample": same_sample,
         "clocks": clk,
         "gpu_launches": int(launches),
-        "ms_each": [round(t, 1) for t in times],
+        "filter": filt_info,
     }
-    if bl is not None:
-        line["batched_learned"] = bl
     if by_level is not None:
         line["by_level"] = by_level
         line["passes_profile"] = {f: {"launches": v[0], "ms": v[1]} for f, v in
@@ -356,66 +498,6 @@ def ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
-
-
-def batched_learned(args, pg, mem, wg, m, q_plain):
-    """Population of K seeds on the workload graph, concurrently on K streams,
-    with the learned move filter trained on logs of plain runs of 262,144-vertex
-    DC-SBMs (seeds 101-104, one pass each)."""
-    from pennsylvaniagpugraphclustering_b200 import graphgen as gg, move_filter as MF
-    t0 = time.perf_counter()
-    xs, ys = [], []
-    for s in (1, 2, 3, 4):
-        h = gg.dcsbm(262144, 100 + s)
-        g2 = pg.weighted_graph(mem, h.rowptr, h.col, h.w, objective=pg.OBJ_WMOD)
-        MF.log_start(mem, capacity=2_000_000, sample_rate=0.25, seed=s)
-        cd = pg.get_objective(mem, g2, pg.OBJ_WMOD, 1.0)
-        pg.run_clustering(mem, g2, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=s)
-        x, y, _ = MF.log_stop(mem, 2_000_000)
-        xs.append(x)
-        ys.append(y)
-        cd.close()
-        g2.close()
-    x = np.concatenate(xs)
-    y = np.concatenate(ys)
-    pos_w = float(min(20.0, (len(y) - y.sum()) / max(y.sum(), 1.0)))
-    params, losses = MF.train(mem, MF.init_params(1), x, y, epochs=6, batch=4096, lr=3e-3, pos_weight=pos_w)
-    thr = MF.threshold_for_recall(mem, params, x, y, recall=args.recall)
-    train_s = time.perf_counter() - t0
-    K = args.batched_learned
-
-    def jobs_for(k):
-        return [dict(graph=wg, objective=pg.OBJ_WMOD, method=pg.METHOD_LEIDEN_PLUS, ex_iters=args.ex_iters,
-                      seed=args.seed + j) for j in range(k)]
-
-    def timed(k, learned):
-        if learned:
-            MF.enable(mem, params, thr)
-        try:
-            # warm-up of the worker streams and their scratch: one cheap pass per job
-            warm = [dict(j, ex_iters=0) for j in jobs_for(k)]
-            pg.batch_run(mem, warm, streams=k)
-            MF.stats(mem, reset=True)
-            t1 = time.perf_counter()
-            res = pg.batch_run(mem, jobs_for(k), streams=k)
-            dt = time.perf_counter() - t1
-            ev, sk = MF.stats(mem)
-        finally:
-            MF.disable(mem)
-        qs = [st["objective"] for _, st in res]
-        return {"value": k * m / dt, "seconds": dt, "modularity_mean": statistics.mean(qs),
-                "modularity_min": min(qs), "passes_mean": statistics.mean(st["passes"] for _, st in res),
-                "sweeps_mean": statistics.mean(st["sweeps"] for _, st in res),
-                "filter_skipped_frac": (sk / max(ev + sk, 1)) if learned else 0.0}
-
-    out = {"unit": UNIT, "population": K, "streams": K, "recall": args.recall, "plain_modularity": q_plain,
-           "train_rows": int(len(y)), "train_seconds": train_s, "final_train_loss": float(losses[-1]),
-           "threshold_logit": thr, "timing": "host wall clock around pggc_batch_run (all streams joined)"}
-    out["learned_1"] = timed(1, True)
-    out["batched_plain"] = timed(K, False)
-    bl = timed(K, True)
-    out.update(bl)
-    return out
 
 
 def main():

@@ -67,7 +67,9 @@ typedef struct pggc_stats {
     int64_t filtered_passes; /* passes run with the filter                                    */
     int64_t exact_passes;    /* exact (unfiltered) passes the judge ran after them              */
     double judge_gain;       /* objective change of those exact passes                         */
-    int64_t fell_back;       /* 1 when judge_gain > PGGC_FILTER_TOLERANCE                      */
+    int64_t fell_back;       /* 1 when the judge's first exact pass gained more than
+                                PGGC_FILTER_TOLERANCE and the run fell back to exact passes
+                                until stable (the plain method)                                */
 } pggc_stats;
 
 /* Modularity the learned filter may give up before its judge counts a fallback
@@ -228,17 +230,18 @@ pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_clu
 /* ---- batched clustering (no counterpart in the reference) ------------------
  * `count` independent run_clustering jobs -- a population of seeds on one graph
  * (the memetic driver's population, app/memetic_clustering.cpp:118-219) or a
- * set of uneven-size graphs -- run concurrently on `streams` CUDA streams of
- * the context's device, one host thread per stream pulling jobs in order.
+ * set of uneven-size graphs -- run concurrently on min(streams, count) CUDA
+ * streams of the context's device, one host thread and one worker context
+ * (stream, memory pool, scratch) per stream pulling jobs in order.
  * Graphs must belong to `ctx`; each job builds its own cluster_data
  * (objective, lambda_mult) and writes labels_out (n int32, host or device per
  * mem_kind), stats and status.  A learned filter enabled on `ctx` applies to
  * every job.  Returns the first failing job's status (its message in
  * pggc_last_error) or PGGC_OK.  Results equal those of sequential
- * pggc_run_clustering calls with the same arguments.  `streams` is an upper
- * bound: one stream per 32 Mi directed edges of the largest graph is used
- * (concurrent runs on graphs that fill the device are slower than sequential
- * ones).  Batch calls on one context are serialised: a second call from
+ * pggc_run_clustering calls with the same arguments.  The workers start after
+ * the work already queued on the context's stream and that stream waits for
+ * all of them, so CUDA events recorded on it around the call bracket the
+ * batch.  Batch calls on one context are serialised: a second call from
  * another host thread waits until the first has finished. */
 typedef struct pggc_batch_job {
     const pggc_graph* graph;
@@ -252,7 +255,46 @@ typedef struct pggc_batch_job {
     pggc_stats stats; /* out */
     int status;       /* out: pggc_status */
 } pggc_batch_job;
+/* streams = 0: the context's tuned batch width (pggc_tune.streams) */
 pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, int streams);
+
+/* ---- kernel-selection knobs and the batch autotuner (no counterpart in the
+ * reference) ------------------------------------------------------------------
+ * The local-move select step picks a kernel per degree class: one thread per
+ * vertex up to thread_max_deg (0, 8, 16 or 32), one warp per vertex up to
+ * warp_max_deg (32 or 127), a block above; warp and block hash tables are
+ * sized for load_factor (0.5 or 0.7).  These replace the reference's fixed
+ * cut-offs (src/header/ordering.h:17-19, the 128-degree team boundary of
+ * src/local_mover.cpp:591-593).  No knob changes any result.  `streams` is the
+ * batch width used when pggc_batch_run is given streams = 0.  Other values
+ * round to the nearest supported one. */
+typedef struct pggc_tune {
+    int thread_max_deg;
+    int warp_max_deg;
+    double load_factor;
+    int streams;
+} pggc_tune;
+pggc_status pggc_tune_set(pggc_context* ctx, const pggc_tune* t);
+pggc_status pggc_tune_get(pggc_context* ctx, pggc_tune* out);
+
+/* One timed configuration of the autotuner: the batch's device time
+ * (seconds, CUDA events on the context stream) and undirected edges / second
+ * over the jobs. */
+typedef struct pggc_tune_trial {
+    pggc_tune config;
+    double seconds;
+    double edges_per_s;
+} pggc_tune_trial;
+/* Tunes the knobs above on a sample batch (the caller's jobs, run as they
+ * are, repeatedly): after one warm-up batch at the current settings, batch
+ * width over {1, 4, 8, 16, 32} (at most `count`), then the thread / warp
+ * degree bounds over {(32,127), (16,127), (8,127), (0,127), (32,32), (8,32)},
+ * then the load factor over {0.5, 0.7}, each step keeping the fastest.  The
+ * best configuration is set on the context and written to *best; the trials
+ * (at most trials_cap) to `trials`, their number to *n_trials.  Job outputs
+ * hold the last trial's results. */
+pggc_status pggc_batch_autotune(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, pggc_tune_trial* trials,
+                                int64_t trials_cap, int64_t* n_trials, pggc_tune* best);
 
 /* ---- memetic driver (app/memetic_clustering.cpp:27-219) -------------------
  * meme_cluster: pop_size pLeiden+ clusterings, then offspring from the

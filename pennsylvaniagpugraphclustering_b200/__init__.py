@@ -5,11 +5,11 @@ contraction, Leiden refinement and the multilevel V-cycles that drive them --
 is hand-written CUDA in ``csrc/`` behind the C ABI of ``include/pggc.h``.
 :mod:`.api` mirrors the reference's host interface on top of that ABI.
 """
-from .api import (NEW_PART, NO_MOVE, NULL_PART, OBJECTIVES, batch_run, build_coarse_graph, cluster_data,
+from .api import (NEW_PART, NO_MOVE, NULL_PART, OBJECTIVES, batch_autotune, batch_run, build_coarse_graph, cluster_data,
                   clustering_methods, cut_signature, graph_from_edges, intersect_clusters, load_graph, load_view, meme_cluster,
                   coarsen_leidenR, constant_potts, generate_orderings, get_objective, local_move, local_move_strict,
-                  memory_store, modularity, normalized_lcc, run_clustering, select_pass, verify_objective,
-                  weighted_graph, write_part)
+                  memory_store, modularity, normalized_lcc, run_clustering, select_pass, tune_get, tune_set,
+                  verify_objective, weighted_graph, write_part)
 from ._lib import (METHOD_LEIDEN, METHOD_LEIDEN_PLUS, METHOD_LOUVAIN, OBJ_CPM, OBJ_LCC, OBJ_MOD, OBJ_NLCC, OBJ_WMOD,
                    DeviceError, InvalidArgument, PggcError)
 
@@ -20,5 +20,5 @@ __all__ = [
     "NO_MOVE", "NEW_PART", "METHOD_LOUVAIN", "METHOD_LEIDEN", "METHOD_LEIDEN_PLUS", "OBJ_MOD", "OBJ_WMOD",
     "OBJ_CPM", "OBJ_NLCC", "OBJ_LCC", "PggcError", "InvalidArgument", "DeviceError", "batch_run", "meme_cluster",
     "intersect_clusters", "cut_signature", "load_graph", "graph_from_edges",
-    "load_view", "write_part",
+    "load_view", "write_part", "batch_autotune", "tune_get", "tune_set",
 ]

@@ -59,6 +59,18 @@ class MemeStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Tune(ctypes.Structure):
+    _fields_ = [("thread_max_deg", ctypes.c_int), ("warp_max_deg", ctypes.c_int), ("load_factor", ctypes.c_double),
+                ("streams", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneTrial(ctypes.Structure):
+    _fields_ = [("config", Tune), ("seconds", ctypes.c_double), ("edges_per_s", ctypes.c_double)]
+
+
 # name -> (restype, argtypes)
 _vp, _i64, _ci, _dbl, _u32, _u64, _flt = (ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float)
@@ -99,6 +111,9 @@ _SIGS = {
     "pggc_filter_enable": (_ci, [_vp, _vp, _flt]),
     "pggc_filter_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _ci]),
     "pggc_batch_run": (_ci, [_vp, _vp, _i64, _ci]),
+    "pggc_tune_set": (_ci, [_vp, ctypes.POINTER(Tune)]),
+    "pggc_tune_get": (_ci, [_vp, ctypes.POINTER(Tune)]),
+    "pggc_batch_autotune": (_ci, [_vp, _vp, _i64, _vp, _i64, ctypes.POINTER(_i64), ctypes.POINTER(Tune)]),
     "pggc_meme_cluster": (_ci, [_vp, _vp, _ci, _dbl, _ci, _i64, _dbl, _u64, _vp, _ci, ctypes.POINTER(MemeStats)]),
     "pggc_intersect_clusters": (_ci, [_vp, _vp, _vp, _i64, _vp, ctypes.POINTER(_i64), _ci]),
     "pggc_cut_signature": (_ci, [_vp, _vp, _vp, _vp, _ci]),

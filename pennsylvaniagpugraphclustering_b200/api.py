@@ -468,14 +468,7 @@ def run_clustering(mem, g, rfd, method=METHOD_LEIDEN_PLUS, ex_iters=0, seed=1, o
     return labels, _stats_dict(st)
 
 
-def batch_run(mem: memory_store, jobs, streams: int = 8):
-    """Run independent clustering jobs concurrently (``pggc_batch_run``).
-
-    ``jobs`` is a list of dicts with keys ``graph`` (a :class:`weighted_graph`
-    of ``mem``), and optionally ``objective`` (default: the graph's),
-    ``lambda_mult`` (1.0), ``method`` (pLeiden+), ``ex_iters`` (0) and
-    ``seed`` (1).  Returns a list of (labels, stats dict) in job order.
-    """
+def _batch_jobs(jobs):
     arr = (L.BatchJob * max(len(jobs), 1))()
     outs = []
     for k, j in enumerate(jobs):
@@ -490,8 +483,52 @@ def batch_run(mem: memory_store, jobs, streams: int = 8):
         arr[k].seed = int(j.get("seed", 1))
         arr[k].labels_out = lab.ctypes.data
         arr[k].mem_kind = MEM_HOST
+    return arr, outs
+
+
+def batch_run(mem: memory_store, jobs, streams: int = 8):
+    """Run independent clustering jobs concurrently (``pggc_batch_run``).
+
+    ``jobs`` is a list of dicts with keys ``graph`` (a :class:`weighted_graph`
+    of ``mem``), and optionally ``objective`` (default: the graph's),
+    ``lambda_mult`` (1.0), ``method`` (pLeiden+), ``ex_iters`` (0) and
+    ``seed`` (1).  ``streams`` = 0 uses the context's tuned batch width.
+    Returns a list of (labels, stats dict) in job order.
+    """
+    arr, outs = _batch_jobs(jobs)
     check(L.lib().pggc_batch_run(mem.handle, ctypes.cast(arr, ctypes.c_void_p), len(jobs), int(streams)))
     return [(outs[k][:jobs[k]["graph"].n], _stats_dict(arr[k].stats)) for k in range(len(jobs))]
+
+
+def tune_get(mem: memory_store) -> dict:
+    """The context's kernel-selection knobs and batch width (``pggc_tune_get``)."""
+    t = L.Tune()
+    check(L.lib().pggc_tune_get(mem.handle, ctypes.byref(t)))
+    return t.as_dict()
+
+
+def tune_set(mem: memory_store, thread_max_deg=32, warp_max_deg=127, load_factor=0.5, streams=4) -> dict:
+    """Set the knobs (``pggc_tune_set``; rounded to supported values); returns them."""
+    t = L.Tune(int(thread_max_deg), int(warp_max_deg), float(load_factor), int(streams))
+    check(L.lib().pggc_tune_set(mem.handle, ctypes.byref(t)))
+    return tune_get(mem)
+
+
+def batch_autotune(mem: memory_store, jobs):
+    """Tune batch width, select degree bounds and table load factor on a sample
+    batch (``pggc_batch_autotune``); the best setting stays on the context.
+    Returns (best dict, [trial dicts])."""
+    arr, _ = _batch_jobs(jobs)
+    cap = 64
+    trials = (L.TuneTrial * cap)()
+    nt = ctypes.c_int64()
+    best = L.Tune()
+    check(L.lib().pggc_batch_autotune(mem.handle, ctypes.cast(arr, ctypes.c_void_p), len(jobs),
+                                      ctypes.cast(trials, ctypes.c_void_p), cap, ctypes.byref(nt),
+                                      ctypes.byref(best)))
+    out = [dict(trials[k].config.as_dict(), seconds=trials[k].seconds, edges_per_s=trials[k].edges_per_s)
+           for k in range(min(nt.value, cap))]
+    return best.as_dict(), out
 
 
 def meme_cluster(mem: memory_store, g: weighted_graph, objective=None, lambda_mult: float = 1.0, pop_size: int = 8,

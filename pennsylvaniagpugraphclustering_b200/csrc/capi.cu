@@ -1,4 +1,5 @@
 // capi.cu -- the extern "C" boundary declared in include/pggc.h.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -872,94 +873,231 @@ pggc_status pggc_run_clustering(pggc_context* ctx, const pggc_graph* g, pggc_clu
     });
 }
 
+// validation shared by the batch entry points
+static void check_batch_jobs(pggc_context* ctx, const pggc_batch_job* jobs, int64_t count) {
+    need(ctx && (count == 0 || jobs), "NULL argument");
+    need(count >= 0, "count must be >= 0");
+    for (i64 k = 0; k < count; k++) {
+        const auto& J = jobs[k];
+        need(J.graph && J.labels_out, "a job has a NULL graph or labels_out");
+        need(J.graph->owner == ctx, "a job's graph belongs to another context");
+        need(J.method >= PGGC_METHOD_LOUVAIN && J.method <= PGGC_METHOD_LEIDEN_PLUS, "unknown method");
+        need(J.objective >= PGGC_OBJ_MOD && J.objective <= PGGC_OBJ_LCC, "unknown objective");
+        check_mem_kind(J.mem_kind);
+    }
+    need(ctx->ctx->filt.mode != 1, "sample logging is not supported in batched runs");
+}
+
+// The batch itself (jobs validated, ctx->batch_mu held by the caller).
+static void batch_impl(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, int streams) {
+    Context& c = *ctx->ctx;
+    if (count == 0) return;
+    c.sync();
+    const int nw = (int)std::min<i64>(streams, count);
+    {
+        std::lock_guard<std::mutex> lk(ctx->workers_mu);
+        while ((int)ctx->workers.size() < nw) ctx->workers.push_back(std::make_unique<Context>(c.device));
+    }
+    // Device-side ordering of the batch against the context stream: the
+    // workers start after the work queued on it so far, and it waits for
+    // every worker, so CUDA events recorded on the context stream around
+    // this call bracket the whole batch on the device.
+    cudaEvent_t start_ev = nullptr;
+    std::vector<cudaEvent_t> done_ev((size_t)nw, nullptr);
+    PGGC_CUDA(cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming));
+    for (auto& e : done_ev) PGGC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    PGGC_CUDA(cudaEventRecord(start_ev, c.stream));
+    std::atomic<i64> next{0};
+    std::vector<std::string> msgs((size_t)count);
+    auto work = [&](int wi) {
+        Context& wc = *ctx->workers[wi];
+        cudaSetDevice(wc.device);
+        cudaStreamWaitEvent(wc.stream, start_ev, 0);
+        // the main context's kernel knobs and learned filter (network,
+        // threshold, counters) are shared read-only
+        wc.tune = c.tune;
+        wc.filt.mode = c.filt.mode;
+        wc.filt.net = c.filt.net;
+        wc.filt.threshold = c.filt.threshold;
+        wc.filt.stats = c.filt.stats;
+        for (;;) {
+            const i64 k = next.fetch_add(1);
+            if (k >= count) break;
+            pggc_batch_job& J = jobs[k];
+            J.status = PGGC_ERR_INTERNAL;
+            try {
+                dispatch(J.graph, [&](auto& gr, auto* vtag) {
+                    using V = std::remove_pointer_t<decltype(vtag)>;
+                    using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
+                    ClusterState<V> cs;
+                    make_cluster_state<W>(wc, gr, J.objective, J.lambda_mult, cs);
+                    Out<i32> lab(wc, J.labels_out, gr.n, J.mem_kind, false);
+                    RunStats rs;
+                    run_clustering<W>(wc, gr, cs, J.method, J.ex_iters, J.seed, lab.p, &rs);
+                    lab.finish();
+                    wc.sync();
+                    fill_stats(&J.stats, rs, cs.get_objective(), cs.obj, cs.label_count);
+                });
+                J.status = PGGC_OK;
+            } catch (const InvalidArg& e) {
+                J.status = PGGC_ERR_INVALID;
+                msgs[k] = e.what();
+            } catch (const DeviceFault& e) {
+                J.status = PGGC_ERR_DEVICE;
+                msgs[k] = e.what();
+            } catch (const CudaError& e) {
+                J.status = PGGC_ERR_CUDA;
+                msgs[k] = e.what();
+            } catch (const std::exception& e) {
+                msgs[k] = e.what();
+            }
+        }
+        wc.filt.mode = 0;
+        wc.filt.net = nullptr;
+        wc.filt.stats = nullptr;
+        cudaEventRecord(done_ev[wi], wc.stream);
+    };
+    std::vector<std::thread> th;
+    for (int wi = 0; wi < nw; wi++) th.emplace_back(work, wi);
+    for (auto& t : th) t.join();
+    for (auto& e : done_ev) {
+        cudaStreamWaitEvent(c.stream, e, 0);
+        cudaEventDestroy(e);
+    }
+    cudaEventDestroy(start_ev);
+    for (i64 k = 0; k < count; k++) {
+        if (jobs[k].status == PGGC_OK) continue;
+        std::string m = "batch job " + std::to_string(k) + ": " + msgs[k];
+        if (jobs[k].status == PGGC_ERR_INVALID) throw InvalidArg(m);
+        if (jobs[k].status == PGGC_ERR_DEVICE) throw DeviceFault(m);
+        if (jobs[k].status == PGGC_ERR_CUDA) throw CudaError(cudaErrorUnknown, m);
+        throw std::runtime_error(m);
+    }
+}
+
 pggc_status pggc_batch_run(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, int streams) {
     return guarded([&] {
-        need(ctx && (count == 0 || jobs), "NULL argument");
-        need(count >= 0 && streams >= 1 && streams <= 64, "count must be >= 0 and streams in [1, 64]");
-        Context& c = *ctx->ctx;
-        for (i64 k = 0; k < count; k++) {
-            const auto& J = jobs[k];
-            need(J.graph && J.labels_out, "a job has a NULL graph or labels_out");
-            need(J.graph->owner == ctx, "a job's graph belongs to another context");
-            need(J.method >= PGGC_METHOD_LOUVAIN && J.method <= PGGC_METHOD_LEIDEN_PLUS, "unknown method");
-            need(J.objective >= PGGC_OBJ_MOD && J.objective <= PGGC_OBJ_LCC, "unknown objective");
-            check_mem_kind(J.mem_kind);
-        }
-        need(c.filt.mode != 1, "sample logging is not supported in batched runs");
-        if (count == 0) return;
+        check_batch_jobs(ctx, jobs, count);
+        need(streams >= 0 && streams <= 64, "streams must be in [0, 64]");
         std::lock_guard<std::mutex> batch_lock(ctx->batch_mu);
-        c.sync();
-        // Runs on large graphs already fill the device; concurrent ones then
-        // contend for L2 and the launch path and were measured slower than
-        // sequential ones (4 x pLeiden+ on a 78M-edge graph: 0.78x).  One
-        // stream per BATCH_EDGES directed edges of the largest graph.
-        constexpr i64 BATCH_EDGES = (i64)32 << 20;
-        i64 max_nnz = 1;
+        batch_impl(ctx, jobs, count, streams == 0 ? ctx->ctx->tune.streams : streams);
+    });
+}
+
+namespace {
+TuneParams tune_from(const pggc_tune& t) {
+    TuneParams p;
+    p.thread_max_deg = t.thread_max_deg >= 24 ? 32 : t.thread_max_deg >= 12 ? 16 : t.thread_max_deg >= 4 ? 8 : 0;
+    p.warp_max_deg = t.warp_max_deg >= 80 ? 127 : 32;
+    p.load = t.load_factor >= 0.6 ? 0.7f : 0.5f;
+    p.streams = std::max(1, std::min(64, t.streams));
+    return p;
+}
+pggc_tune tune_to(const TuneParams& p) {
+    pggc_tune t;
+    t.thread_max_deg = p.thread_max_deg;
+    t.warp_max_deg = p.warp_max_deg;
+    t.load_factor = p.load;
+    t.streams = p.streams;
+    return t;
+}
+}  // namespace
+
+pggc_status pggc_tune_set(pggc_context* ctx, const pggc_tune* t) {
+    return guarded([&] {
+        need(ctx && t, "NULL argument");
+        ctx->ctx->tune = tune_from(*t);
+    });
+}
+
+pggc_status pggc_tune_get(pggc_context* ctx, pggc_tune* out) {
+    return guarded([&] {
+        need(ctx && out, "NULL argument");
+        *out = tune_to(ctx->ctx->tune);
+    });
+}
+
+pggc_status pggc_batch_autotune(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, pggc_tune_trial* trials,
+                                int64_t trials_cap, int64_t* n_trials, pggc_tune* best) {
+    return guarded([&] {
+        check_batch_jobs(ctx, jobs, count);
+        need(count > 0, "the autotuner needs at least one job");
+        need(trials_cap >= 0 && (trials_cap == 0 || trials), "invalid trial buffer");
+        std::lock_guard<std::mutex> batch_lock(ctx->batch_mu);
+        Context& c = *ctx->ctx;
+        double edges = 0;
         for (i64 k = 0; k < count; k++)
-            max_nnz = std::max<i64>(max_nnz, jobs[k].graph->is_float() ? jobs[k].graph->gf->nnz : jobs[k].graph->gi->nnz);
-        const i64 by_size = std::max<i64>(1, BATCH_EDGES / max_nnz);
-        const int nw = (int)std::min<i64>(std::min<i64>(streams, count), by_size);
-        {
-            std::lock_guard<std::mutex> lk(ctx->workers_mu);
-            while ((int)ctx->workers.size() < nw) ctx->workers.push_back(std::make_unique<Context>(c.device));
-        }
-        std::atomic<i64> next{0};
-        std::vector<std::string> msgs((size_t)count);
-        auto work = [&](int wi) {
-            Context& wc = *ctx->workers[wi];
-            cudaSetDevice(wc.device);
-            // the main context's learned filter (network, threshold, counters) is shared read-only
-            wc.filt.mode = c.filt.mode;
-            wc.filt.net = c.filt.net;
-            wc.filt.threshold = c.filt.threshold;
-            wc.filt.stats = c.filt.stats;
-            for (;;) {
-                const i64 k = next.fetch_add(1);
-                if (k >= count) break;
-                pggc_batch_job& J = jobs[k];
-                J.status = PGGC_ERR_INTERNAL;
-                try {
-                    dispatch(J.graph, [&](auto& gr, auto* vtag) {
-                        using V = std::remove_pointer_t<decltype(vtag)>;
-                        using W = std::conditional_t<std::is_same<V, double>::value, float, i32>;
-                        ClusterState<V> cs;
-                        make_cluster_state<W>(wc, gr, J.objective, J.lambda_mult, cs);
-                        Out<i32> lab(wc, J.labels_out, gr.n, J.mem_kind, false);
-                        RunStats rs;
-                        run_clustering<W>(wc, gr, cs, J.method, J.ex_iters, J.seed, lab.p, &rs);
-                        lab.finish();
-                        wc.sync();
-                        fill_stats(&J.stats, rs, cs.get_objective(), cs.obj, cs.label_count);
-                    });
-                    J.status = PGGC_OK;
-                } catch (const InvalidArg& e) {
-                    J.status = PGGC_ERR_INVALID;
-                    msgs[k] = e.what();
-                } catch (const DeviceFault& e) {
-                    J.status = PGGC_ERR_DEVICE;
-                    msgs[k] = e.what();
-                } catch (const CudaError& e) {
-                    J.status = PGGC_ERR_CUDA;
-                    msgs[k] = e.what();
-                } catch (const std::exception& e) {
-                    msgs[k] = e.what();
-                }
+            edges += 0.5 * (double)(jobs[k].graph->is_float() ? jobs[k].graph->gf->nnz : jobs[k].graph->gi->nnz);
+        cudaEvent_t e0, e1;
+        PGGC_CUDA(cudaEventCreate(&e0));
+        PGGC_CUDA(cudaEventCreate(&e1));
+        i64 nt = 0;
+        auto trial = [&](const TuneParams& p) -> double {
+            c.tune = p;
+            PGGC_CUDA(cudaEventRecord(e0, c.stream));
+            batch_impl(ctx, jobs, count, p.streams);
+            PGGC_CUDA(cudaEventRecord(e1, c.stream));
+            PGGC_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PGGC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const double sec = ms / 1000.0;
+            if (nt < trials_cap) {
+                trials[nt].config = tune_to(p);
+                trials[nt].seconds = sec;
+                trials[nt].edges_per_s = sec > 0 ? edges / sec : 0;
             }
-            wc.filt.mode = 0;
-            wc.filt.net = nullptr;
-            wc.filt.stats = nullptr;
+            nt++;
+            return sec;
         };
-        std::vector<std::thread> th;
-        for (int wi = 0; wi < nw; wi++) th.emplace_back(work, wi);
-        for (auto& t : th) t.join();
-        for (i64 k = 0; k < count; k++) {
-            if (jobs[k].status == PGGC_OK) continue;
-            std::string m = "batch job " + std::to_string(k) + ": " + msgs[k];
-            if (jobs[k].status == PGGC_ERR_INVALID) throw InvalidArg(m);
-            if (jobs[k].status == PGGC_ERR_DEVICE) throw DeviceFault(m);
-            if (jobs[k].status == PGGC_ERR_CUDA) throw CudaError(cudaErrorUnknown, m);
-            throw std::runtime_error(m);
+        try {
+            TuneParams cur = c.tune;
+            // warm-up at the widest batch width tried (creates the worker contexts)
+            cur.streams = (int)std::min<i64>(32, count);
+            c.tune = cur;
+            batch_impl(ctx, jobs, count, cur.streams);
+            TuneParams bestp = cur;
+            double best_s = 1e300;
+            auto consider = [&](TuneParams p) {
+                const double sec = trial(p);
+                if (sec < best_s) {
+                    best_s = sec;
+                    bestp = p;
+                }
+            };
+            std::vector<int> widths;
+            for (int sw : {1, 4, 8, 16, 32}) {
+                const int w = (int)std::min<i64>(sw, count);
+                if (std::find(widths.begin(), widths.end(), w) != widths.end()) continue;
+                widths.push_back(w);
+                TuneParams p = cur;
+                p.streams = w;
+                consider(p);
+            }
+            cur = bestp;
+            const int th[6][2] = {{32, 127}, {16, 127}, {8, 127}, {0, 127}, {32, 32}, {8, 32}};
+            for (auto& t : th) {
+                TuneParams p = cur;
+                p.thread_max_deg = t[0];
+                p.warp_max_deg = t[1];
+                if (p.thread_max_deg == cur.thread_max_deg && p.warp_max_deg == cur.warp_max_deg) continue;
+                consider(p);
+            }
+            cur = bestp;
+            {
+                TuneParams p = cur;
+                p.load = cur.load >= 0.7f ? 0.5f : 0.7f;
+                consider(p);
+            }
+            c.tune = bestp;
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
         }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (n_trials) *n_trials = nt;
+        if (best) *best = tune_to(c.tune);
     });
 }
 

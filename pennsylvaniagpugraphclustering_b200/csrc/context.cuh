@@ -27,8 +27,20 @@ struct ProfStat {
     double bytes = 0.0;
 };
 
+// Kernel-selection knobs of the local-move select step.  Results do not
+// depend on them (every select kernel aggregates exact sums and applies the
+// same argmax order); they only move work between kernels.  Set by
+// pggc_tune_set or by the batch autotuner.
+struct TuneParams {
+    int thread_max_deg = 32;  // 0, 8, 16 or 32: one thread per vertex up to this degree
+    int warp_max_deg = 127;   // 32 or 127: one warp per vertex up to this degree, a block above
+    float load = 0.5f;        // load-factor bound of the warp / block hash tables: 0.5 or 0.7
+    int streams = 4;          // batch width for batch calls that pass streams = 0
+};
+
 struct Context {
     int device = 0;
+    TuneParams tune;
     cudaStream_t stream = nullptr;
     int* d_err = nullptr;          // DevErr latched by kernels
     void* h_pin = nullptr;         // pinned scratch for scalar readbacks

@@ -396,25 +396,32 @@ void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Trait
         one(true);
     }
     if (ctx.filt.mode == 2) {
-        // Judge of the learned move filter: exact (unfiltered) improvement
-        // passes from the filtered result while the objective rises -- at least
-        // one.  Whatever they gain is what the filter gave up; the run ends on
-        // the exact passes' result either way (the plain method's fallback),
-        // and a gain above FILTER_TOLERANCE is reported as a fallback.  The
-        // objective is cluster_data's FP64 value from exact int64 / FP64 sums
-        // (the verify_obj arithmetic of app/verify_objective.cpp:108-135).
+        // Judge of the learned move filter: one exact (unfiltered) improvement
+        // pass from the filtered result.  What it gains is what the filter gave
+        // up; above FILTER_TOLERANCE the run falls back to the plain method --
+        // exact passes from there while the objective rises -- and reports
+        // the fallback.  The run ends on the exact passes' result either way.
+        // The objective is cluster_data's FP64 value from exact int64 / FP64
+        // sums (the verify_obj arithmetic of app/verify_objective.cpp:108-135).
         acc.filtered_passes = acc.passes;
         const double q_filtered = cs.get_objective();
         ctx.filt.mode = 0;
+        bool fell_back = false;
         try {
-            double prev = q_filtered;
-            while (true) {
-                copy_d2d(ctx, con.p, part.p, n);
-                one(true);
-                acc.exact_passes++;
-                const double q = cs.get_objective();
-                if (!(q > prev)) break;
-                prev = q;
+            copy_d2d(ctx, con.p, part.p, n);
+            one(true);
+            acc.exact_passes++;
+            fell_back = cs.get_objective() - q_filtered > FILTER_TOLERANCE;
+            if (fell_back) {
+                double prev = cs.get_objective();
+                while (true) {
+                    copy_d2d(ctx, con.p, part.p, n);
+                    one(true);
+                    acc.exact_passes++;
+                    const double q = cs.get_objective();
+                    if (!(q > prev)) break;
+                    prev = q;
+                }
             }
         } catch (...) {
             ctx.filt.mode = 2;
@@ -422,7 +429,7 @@ void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Trait
         }
         ctx.filt.mode = 2;
         acc.judge_gain = cs.get_objective() - q_filtered;
-        acc.fell_back = acc.judge_gain > FILTER_TOLERANCE ? 1 : 0;
+        acc.fell_back = fell_back ? 1 : 0;
     }
     copy_d2d(ctx, labels_out, part.p, n);
     if (rs) *rs = acc;

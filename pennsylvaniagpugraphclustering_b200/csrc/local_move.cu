@@ -105,7 +105,14 @@ struct SelArgs {
     int* err;
     unsigned long long* prof;  // algorithmic-byte counter (profiling only)
     u32 probe_cap;             // fault-injection cap on hash probes (0: none)
+    float inv_load;            // hash-table slots per distinct key (1 / load factor): 2 or 1/0.7
 };
+
+// table slots for up to U distinct keys at the tuned load factor (a power of two)
+template <class W>
+__device__ __forceinline__ u32 sel_table_slots(const SelArgs<W>& a, i64 U) {
+    return next_pow2_u32((u32)ceilf((float)U * a.inv_load));
+}
 
 // algorithmic bytes of one select evaluation: list entry + dest read, then
 // rowptr pair, vtx_w, part, pval, D[part], dest/gain writes, and per edge the
@@ -325,7 +332,7 @@ __global__ void __launch_bounds__(SELW_WARPS * 32) k_select_warp(SelArgs<W> a, R
             V s = peer_sum<W>(a, peers, wr, keep, leader);
             if (leader) sel_eval<W, CON>(a, vc, c, s, best);
         } else {
-            u32 T = next_pow2_u32((u32)(2 * (e - b)));
+            u32 T = sel_table_slots(a, e - b);
             i32* keys = tk[w];
             V* vals = tv[w];
             for (u32 s = l; s < T; s += 32) {
@@ -657,8 +664,8 @@ __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg
             }
         } else {
             i64 U = min(e - b, *a.label_count);
-            u32 T = next_pow2_u32((u32)(2 * U));
-            if (OVF && T > (u32)gcap) T = (u32)gcap;
+            u32 T = sel_table_slots(a, U);
+            if (T > (u32)gcap) T = (u32)gcap;
             for (u32 s = threadIdx.x; s < T; s += THREADS) {
                 keys[s] = -1;
                 vals[s] = V(0);
@@ -1816,6 +1823,7 @@ struct Mover {
         a.probe_cap = ctx.probe_cap;
         a.keys32 = cap < ((i64)1 << 29) ? 1 : 0;
         a.dense = 0;
+        a.inv_load = ctx.tune.load >= 0.7f ? 1.0f / 0.7f : 2.0f;
         return a;
     }
 
@@ -1823,36 +1831,51 @@ struct Mover {
 
     template <bool CON>
     void launch_select_t(SelArgs<W> a) {
+        // degree classes 0..2 (<= 8, 16, 32) go to the thread kernels up to the
+        // tuned thread bound, the rest below 128 to the warp kernel up to the
+        // tuned warp bound, and everything above to the block kernels
+        const TuneParams& tp = ctx.tune;
+        const int tcls = tp.thread_max_deg >= 32 ? 3 : tp.thread_max_deg >= 16 ? 2 : tp.thread_max_deg >= 8 ? 1 : 0;
+        const int wend = tp.warp_max_deg >= 127 ? 4 : 3;  // first class after the warp kernel's
         if (ord.off_large > 0) {
             ProfScope ps(ctx, "select_warp");
             a.prof = ctx.prof_counter("select_warp");
-            int grid_g = grid_for(ctx, ceil_div(cls.count, 32), 1, 16);
             int grid_t = grid_for(ctx, ceil_div(cls.count, 256), 1, 16);
-            k_select_thr<W, CON, 8><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 0);
-            PGGC_LAUNCH_CHECK();
-            k_select_thr<W, CON, 16><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 1);
-            PGGC_LAUNCH_CHECK();
-            k_select_thr<W, CON, 32><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 2);
-            PGGC_LAUNCH_CHECK();
-            int grid = grid_for(ctx, ceil_div(ord.off_large, SELW_WARPS), 1, 16);
-            k_select_warp<W, CON><<<grid, SELW_WARPS * 32, 0, ctx.stream>>>(a, dev_range(cls.list, cls.off + 3,
-                                                                                          cls.off + 4));
-            PGGC_LAUNCH_CHECK();
+            if (tcls > 0) {
+                k_select_thr<W, CON, 8><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 0);
+                PGGC_LAUNCH_CHECK();
+            }
+            if (tcls > 1) {
+                k_select_thr<W, CON, 16><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 1);
+                PGGC_LAUNCH_CHECK();
+            }
+            if (tcls > 2) {
+                k_select_thr<W, CON, 32><<<grid_t, 256, 0, ctx.stream>>>(a, cls.list, cls.off, 2);
+                PGGC_LAUNCH_CHECK();
+            }
+            if (tcls < wend) {
+                int grid = grid_for(ctx, ceil_div(ord.off_large, SELW_WARPS), 1, 16);
+                k_select_warp<W, CON><<<grid, SELW_WARPS * 32, 0, ctx.stream>>>(
+                    a, dev_range(cls.list, cls.off + tcls, cls.off + wend));
+                PGGC_LAUNCH_CHECK();
+            }
         }
         i64 nb = n - ord.off_large;
-        if (nb > 0) {
+        if (nb > 0 || (wend < 4 && ord.off_large > 0)) {
             ProfScope ps(ctx, "select_block");
             a.prof = ctx.prof_counter("select_block");
-            // class 4 (degree <= 1024): 2048-slot tables, 8 blocks of 256 per SM;
-            // class 5 (degree <= 4096): 8192-slot tables, 2 blocks of 512 per SM
+            // classes from the warp bound to 4 (degree <= 1024): 2048-slot
+            // tables, 8 blocks of 256 per SM; class 5 (degree <= 4096):
+            // 8192-slot tables, 2 blocks of 512 per SM
             const size_t slot = sizeof(V) + sizeof(i32);
-            const i64 n4 = std::min<i64>(nb, (i64)ctx.num_sms * 8), n5 = std::min<i64>(nb, (i64)ctx.num_sms * 2);
+            const i64 nb4 = wend < 4 ? n : nb;
+            const i64 n4 = std::min<i64>(nb4, (i64)ctx.num_sms * 8), n5 = std::min<i64>(nb, (i64)ctx.num_sms * 2);
             // with at most as many labels as table slots, the table is indexed
             // by cluster id directly (no probing, no keys)
             SelArgs<W> a4 = a;
             a4.dense = label_bound_host <= 2048 ? 1 : 0;
             k_select_block<W, CON, false, 256><<<(int)n4, 256, slot * 2048, ctx.stream>>>(
-                a4, dev_range(cls.list, cls.off + 4, cls.off + 5), nullptr, nullptr, 2048);
+                a4, dev_range(cls.list, cls.off + wend, cls.off + 5), nullptr, nullptr, 2048);
             PGGC_LAUNCH_CHECK();
             if (ord.max_deg > 1024) {
                 SelArgs<W> a5 = a;

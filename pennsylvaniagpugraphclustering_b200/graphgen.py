@@ -124,3 +124,27 @@ def dcsbm_4m(seed: int = 1, n: int = 4194304) -> HostGraph:
 def rmat24(seed: int = 1, scale: int = 24) -> HostGraph:
     """Contraction stress workload: R-MAT scale 24, edge factor 16, a=0.57, b=c=0.19."""
     return rmat(scale, 16, 0.57, 0.19, 0.19, seed)
+
+
+def sbm_population_params(count: int = 256, seed: int = 1, n_lo: int = 1000, n_hi: int = 200000,
+                          b_lo: int = 8, b_hi: int = 512):
+    """Sizes of the batched workload's uneven-size SBM population: vertex
+    counts log-uniform in [n_lo, n_hi], block counts log-uniform in
+    [b_lo, b_hi] (at most n // 16 so that every block holds at least 16
+    vertices, enough for expected intra-block degree 12), and one generator
+    seed per graph.  Returns a list of (n, blocks, seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        b = int(round(np.exp(rng.uniform(np.log(b_lo), np.log(b_hi)))))
+        b = max(1, min(b, n // 16))
+        out.append((n, b, int(rng.integers(1, 1 << 31))))
+    return out
+
+
+def sbm_population(count: int = 256, seed: int = 1, deg_in: float = 12.0, deg_out: float = 3.0):
+    """The batched workload's population: `count` independent planted-partition
+    SBMs (unit weights, expected intra / inter degree 12 / 3) with the sizes of
+    :func:`sbm_population_params`."""
+    return [sbm(n, b, deg_in, deg_out, s) for n, b, s in sbm_population_params(count, seed)]

@@ -56,3 +56,60 @@ def test_batch_reports_the_failing_job(mem):
     with pytest.raises(Exception) as ei:
         pg.batch_run(mem, jobs, streams=2)
     assert "method" in str(ei.value)
+
+
+KNOBS = [dict(thread_max_deg=32, warp_max_deg=127, load_factor=0.5),
+         dict(thread_max_deg=8, warp_max_deg=127, load_factor=0.7),
+         dict(thread_max_deg=0, warp_max_deg=127, load_factor=0.5),
+         dict(thread_max_deg=16, warp_max_deg=32, load_factor=0.7),
+         dict(thread_max_deg=8, warp_max_deg=32, load_factor=0.5)]
+
+
+@pytest.mark.parametrize("name", ["dcsbm_wmod", "rmat12", "hub"])
+def test_kernel_knobs_do_not_change_results(mem, name):
+    """Every select-kernel split and table load factor the autotuner can pick
+    gives the default's labels and objective bit for bit."""
+    if name == "dcsbm_wmod":
+        hg, obj = G.small_dcsbm(seed=2), pg.OBJ_WMOD
+    elif name == "rmat12":
+        hg, obj = G.small_rmat(seed=2), pg.OBJ_MOD
+    else:
+        hg, obj = G.hub_graph(), pg.OBJ_WMOD
+    g = pg.weighted_graph(mem, hg.rowptr, hg.col, hg.w if obj == pg.OBJ_WMOD else None, objective=obj)
+    saved = pg.tune_get(mem)
+    ref = None
+    try:
+        for kn in KNOBS:
+            got = pg.tune_set(mem, streams=saved["streams"], **kn)
+            assert got["thread_max_deg"] == kn["thread_max_deg"]
+            lab, st = _seq(mem, g, obj, pg.METHOD_LEIDEN_PLUS, 1, 5)
+            if ref is None:
+                ref = (lab, st)
+            else:
+                assert np.array_equal(lab, ref[0]), kn
+                assert st["objective"] == ref[1]["objective"]
+    finally:
+        pg.tune_set(mem, **{k: saved[k] for k in ("thread_max_deg", "warp_max_deg", "load_factor", "streams")})
+
+
+def test_autotuner_picks_the_fastest_trial_and_keeps_results(mem):
+    pop = gg.sbm_population(12, 3)
+    graphs = [pg.weighted_graph(mem, h.rowptr, h.col, None, objective=pg.OBJ_MOD) for h in pop]
+    jobs = [dict(graph=g, objective=pg.OBJ_MOD, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=k + 1)
+            for k, g in enumerate(graphs)]
+    saved = pg.tune_get(mem)
+    try:
+        best, trials = pg.batch_autotune(mem, jobs)
+        assert len(trials) >= 9
+        fastest = min(trials, key=lambda t: t["seconds"])
+        for k in ("thread_max_deg", "warp_max_deg", "load_factor", "streams"):
+            assert best[k] == fastest[k]
+        assert pg.tune_get(mem) == best
+        # streams = 0: the tuned width; results equal sequential runs
+        res = pg.batch_run(mem, jobs, streams=0)
+        for j, (lab, st) in zip(jobs, res):
+            lo, so = _seq(mem, j["graph"], pg.OBJ_MOD, pg.METHOD_LEIDEN_PLUS, 0, j["seed"])
+            assert np.array_equal(lab, lo)
+            assert st["objective"] == so["objective"]
+    finally:
+        pg.tune_set(mem, **{k: saved[k] for k in ("thread_max_deg", "warp_max_deg", "load_factor", "streams")})

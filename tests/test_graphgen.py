@@ -55,3 +55,20 @@ def test_dcsbm_shape_scaled():
     assert 17.0 < deg.mean() < 21.0
     assert deg.min() >= 1
     assert g.w.min() >= 0.5 and g.w.max() < 1.5
+
+
+def test_sbm_population_shapes():
+    params = gg.sbm_population_params(256, 1)
+    assert len(params) == 256
+    ns = np.array([p[0] for p in params])
+    bs = np.array([p[1] for p in params])
+    assert ns.min() >= 1000 and ns.max() <= 200000
+    assert np.all(bs >= 1) and np.all(bs <= 512) and np.all(ns // bs >= 16)
+    # log-uniform sizes: about half the graphs below the geometric midpoint
+    mid = np.sqrt(1000 * 200000)
+    assert 0.35 < np.mean(ns < mid) < 0.65
+    assert params == gg.sbm_population_params(256, 1)
+    pop = gg.sbm_population(3, 2)
+    for g, (n, b, s) in zip(pop, gg.sbm_population_params(3, 2)):
+        assert g.n == n
+        check_csr(g)
