@@ -86,6 +86,12 @@ def parse():
                     help="profiled run also splits each kernel family by multilevel level (adds 'by_level')")
     ap.add_argument("--ex-iters", type=int, default=-1,
                     help="pLeiden+ passes after the first (-1: until the objective stops rising)")
+    ap.add_argument("--workload", default="dcsbm4m", choices=["dcsbm4m", "rmat24", "sbm65k", "sbm-population"],
+                    help="dcsbm4m: the headline line (batched+learned vs plain pLeiden+); rmat24: plain pLouvain "
+                         "on R-MAT scale 24 (contraction stress); sbm65k: plain pLouvain on the planted SBM; "
+                         "sbm-population: 256 uneven SBMs, batched (autotuned) vs sequential pLeiden+")
+    ap.add_argument("--population", type=int, default=256, help="sbm-population: number of graphs")
+    ap.add_argument("--rmat-scale", type=int, default=24)
     return ap.parse_args()
 
 
@@ -500,12 +506,200 @@ def ours(args):
         dist.destroy_process_group()
 
 
+def _families(lib, _lib, mem):
+    fam = {}
+    for f in DOMINANT_FAMILIES + SUB_PHASES:
+        n_l, t_ms, by = (_lib.ctypes.c_int64(), _lib.ctypes.c_double(), _lib.ctypes.c_double())
+        _lib.check(lib.pggc_profile_read(mem.handle, f.encode(), _lib.ctypes.byref(n_l), _lib.ctypes.byref(t_ms),
+                                         _lib.ctypes.byref(by)))
+        fam[f] = (n_l.value, t_ms.value, by.value)
+    return fam
+
+
+def _roofline(fam):
+    dom = max((f for f in DOMINANT_FAMILIES if fam[f][2] > 0), key=lambda f: fam[f][1], default=None)
+    if dom is None:
+        return None
+    peak, peak_kind = peaks()
+    nl, tms, by = fam[dom]
+    achieved = by / (tms / 1000.0) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_for(dom),
+            "algorithmic_bytes_per_launch": by / max(nl, 1), "avg_launch_ms": tms / max(nl, 1), "launches": nl}
+
+
+def plain_workload(args):
+    """One named workload, plain method, single stream: R-MAT scale 24 pLouvain
+    (the contraction stress: hub rows above 15,000 edges, large hash merges) or
+    the planted SBM n = 65,536 pLouvain.  K timed runs with CUDA events, a
+    profiled run for the kernel families and the roofline, an e2e run from host
+    buffers, and the oracle port on the CPU (the SBM in full; R-MAT at scale
+    20, same generator parameters)."""
+    import torch
+    import pennsylvaniagpugraphclustering_b200 as pg
+    from pennsylvaniagpugraphclustering_b200 import _lib, graphgen as gg
+    torch.cuda.set_device(0)
+    if args.workload == "rmat24":
+        g = gg.rmat(args.rmat_scale, 16, 0.57, 0.19, 0.19, args.seed)
+        desc = (f"plain pLouvain (ex_iters=0), Mod, R-MAT scale {args.rmat_scale} edge factor 16 a=0.57 b=c=0.19 "
+                f"d=0.05, symmetrised, deduplicated, no self-loops, unit weights, int64 offsets")
+        cpu_graph = lambda: gg.rmat(min(20, args.rmat_scale), 16, 0.57, 0.19, 0.19, args.seed)
+    else:
+        g = gg.planted_sbm_65k(args.seed)
+        desc = ("plain pLouvain (ex_iters=0), Mod, planted-partition SBM n=65,536 in 64 blocks of 1,024, expected "
+                "degrees 16/4, unit weights")
+        cpu_graph = lambda: g
+    mem = pg.memory_store(0)
+    stream = torch.cuda.ExternalStream(mem.stream(), device=torch.device("cuda", 0))
+    lib = _lib.lib()
+    wg = pg.weighted_graph(mem, g.rowptr, g.col, None, objective=pg.OBJ_MOD)
+    labels = torch.empty(max(g.n, 1), dtype=torch.int32, device="cuda:0")
+
+    def run():
+        cd = pg.get_objective(mem, wg, pg.OBJ_MOD, 1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, st = pg.run_clustering(mem, wg, cd, method=pg.METHOD_LOUVAIN, ex_iters=0, seed=args.seed, out=labels)
+        e1.record(stream)
+        e1.synchronize()
+        cd.close()
+        return e0.elapsed_time(e1), st
+
+    for _ in range(args.warmup):
+        run()
+    clocks = ClockSampler(0)
+    clocks.start()
+    l0 = lib.pggc_launch_count()
+    times, st = [], None
+    for _ in range(max(1, args.steps)):
+        ms, st = run()
+        times.append(ms)
+    launches = lib.pggc_launch_count() - l0
+    clk = clocks.stop()
+    _lib.check(lib.pggc_profile_reset(mem.handle))
+    _lib.check(lib.pggc_profile_enable(mem.handle, 1))
+    run()
+    _lib.check(lib.pggc_profile_enable(mem.handle, 0))
+    fam = _families(lib, _lib, mem)
+    q, _ = pg.verify_objective(mem, wg, labels[:g.n].cpu().numpy(), pg.OBJ_MOD)
+    # e2e from host buffers
+    host = np.empty(g.n, np.int32)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g2 = pg.weighted_graph(mem, g.rowptr, g.col, None, objective=pg.OBJ_MOD)
+    cd2 = pg.get_objective(mem, g2, pg.OBJ_MOD, 1.0)
+    pg.run_clustering(mem, g2, cd2, method=pg.METHOD_LOUVAIN, ex_iters=0, seed=args.seed, out=host)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    cd2.close()
+    g2.close()
+    ms = statistics.mean(times)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        h = cpu_graph()
+        og = O.Graph(h.rowptr, h.col, None, objective=O.OBJ_MOD)
+        cdo = O.ClusterData(og, O.OBJ_MOD, 1.0)
+        t0 = time.perf_counter()
+        _, so = O.run_clustering(og, cdo, method=O.METHOD_LOUVAIN, ex_iters=0, seed=args.seed)
+        dt = time.perf_counter() - t0
+        cpu = {"value": h.m / dt, "unit": UNIT, "cores": int(O.lib().orc_num_threads()), "kind": "port",
+               "modularity": so.objective,
+               "sample": f"{'the same graph' if h is g else f'R-MAT scale {min(20, args.rmat_scale)}'} "
+                         f"(n={h.n}, m={h.m}); one pLouvain run, {dt:.3f} s; modularity {so.objective:.6f}"}
+    line = {"metric": f"Louvain edges/s ({args.workload})", "value": g.m / (ms / 1000.0), "unit": UNIT,
+            "n_gpus": 1, "steps": len(times), "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": desc, "n": g.n, "m_undirected": g.m, "nnz": g.nnz,
+                       "max_degree": int(np.diff(g.rowptr).max()), "modularity": st["objective"],
+                       "verify_modularity": q, "levels": st["levels"], "labels": st["label_count"],
+                       "l2": "inputs larger than L2" if g.nnz * 4 > 126e6 else "inputs smaller than L2"},
+            "e2e": {"value": g.m / (e2e_ms / 1000.0), "unit": UNIT,
+                    "h2d_bytes_per_step": int(g.rowptr.nbytes + g.col.nbytes), "d2h_bytes_per_step": int(host.nbytes),
+                    "ms_per_step": e2e_ms},
+            "roofline": _roofline(fam),
+            "kernel_families": {f: {"launches": v[0], "ms": v[1], "alg_bytes": v[2]} for f, v in fam.items()},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
+            "ms_each": [round(t, 2) for t in times]}
+    print(json.dumps(line), flush=True)
+
+
+def population(args):
+    """The batched workload's uneven-size population: `--population` planted
+    SBMs (n log-uniform in [1,000, 200,000], 8-512 blocks, expected degrees
+    12 / 3, unit weights), one pLeiden+ pass each.  Sequential runs on one
+    stream against one batch with the autotuned width and kernel knobs (the
+    autotuner runs first on every 8th graph)."""
+    import torch
+    import pennsylvaniagpugraphclustering_b200 as pg
+    from pennsylvaniagpugraphclustering_b200 import _lib, graphgen as gg
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    pop = gg.sbm_population(args.population, args.seed)
+    gen_s = time.perf_counter() - t0
+    mem = pg.memory_store(0)
+    stream = torch.cuda.ExternalStream(mem.stream(), device=torch.device("cuda", 0))
+    graphs = [pg.weighted_graph(mem, h.rowptr, h.col, None, objective=pg.OBJ_MOD) for h in pop]
+    m_total = sum(h.m for h in pop)
+    jobs = [dict(graph=g, objective=pg.OBJ_MOD, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=k + 1)
+            for k, g in enumerate(graphs)]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def sequential():
+        res = []
+        for j in jobs:
+            cd = pg.get_objective(mem, j["graph"], pg.OBJ_MOD, 1.0)
+            res.append(pg.run_clustering(mem, j["graph"], cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0,
+                                         seed=j["seed"])[1])
+            cd.close()
+        return res
+
+    sequential()  # warm-up (per-graph caches, pools)
+    ms_seq, seq = timed(sequential)
+    best, trials = pg.batch_autotune(mem, jobs[::8])
+    pg.batch_run(mem, jobs, streams=0)  # warm-up at the tuned width
+    ms_bat, bat = timed(lambda: pg.batch_run(mem, jobs, streams=0))
+    same = all(a["objective"] == b["objective"] for a, (_, b) in zip(seq, bat))
+    default_knobs = {"thread_max_deg": 32, "warp_max_deg": 127, "load_factor": 0.5}
+    pg.tune_set(mem, streams=best["streams"], **default_knobs)
+    ms_def, _ = timed(lambda: pg.batch_run(mem, jobs, streams=0))
+    line = {"metric": "Leiden edges/s, batched vs sequential (uneven SBM population)",
+            "value": m_total / (ms_bat / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": len(jobs), "warmup": 1,
+            "ms_per_step": ms_bat / len(jobs), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64", "data": "synthetic",
+            "config": {"workload": f"{len(pop)} planted SBMs, n log-uniform in [1000, 200000], 8-512 blocks, "
+                                   f"expected degrees 12/3, unit weights, Mod, one pLeiden+ pass each",
+                       "vertices_total": int(sum(h.n for h in pop)), "m_total": int(m_total),
+                       "generator_seconds": gen_s},
+            "sequential": {"value": m_total / (ms_seq / 1000.0), "ms": ms_seq},
+            "batched": {"value": m_total / (ms_bat / 1000.0), "ms": ms_bat, "tuned": best},
+            "batched_default_knobs": {"value": m_total / (ms_def / 1000.0), "ms": ms_def},
+            "batched_over_sequential": ms_seq / ms_bat, "identical_objectives": same,
+            "autotune_trials": trials}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
-    else:
+    elif args.workload == "dcsbm4m":
         ours(args)
+    elif args.workload == "sbm-population":
+        population(args)
+    else:
+        plain_workload(args)
 
 
 if __name__ == "__main__":
