@@ -76,6 +76,7 @@ def lib():
         L.orc_murmur3.argtypes = [u32]
         L.orc_murmur3.restype = u32
         L.orc_num_threads.restype = ci
+        L.orc_set_afterburner_reference_order.argtypes = [ci]
         L.orc_intersect.argtypes = [vp, vp, i64, vp]
         L.orc_intersect.restype = i64
         L.orc_signature.argtypes = [vp, vp, vp]
@@ -88,6 +89,14 @@ def lib():
         L.orc_last_error.argtypes = []
         _LIB = L
     return _LIB
+
+
+def set_afterburner_reference_order(on: bool) -> None:
+    """Test switch: sum the afterburner's change and the strict prefix's gains
+    in FP32 in the reference's order (on) instead of the canonical FP64
+    association the CUDA library uses (off, the default) -- for step-by-step
+    comparisons with the reference's own code (oracle/ref.py)."""
+    lib().orc_set_afterburner_reference_order(1 if on else 0)
 
 
 class MemeStats(ctypes.Structure):

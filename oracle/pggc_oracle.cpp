@@ -65,6 +65,12 @@ constexpr i32 NULL_PART = -1;
 constexpr i32 NO_MOVE = -3;
 constexpr i32 NEW_PART = -4;
 constexpr float AFTERBURNER_EPS = 0.1f;
+// Test switch: 0 (default) sums the afterburner's change and the strict
+// prefix's gains canonically in FP64, as the CUDA library does; 1 accumulates
+// them in FP32 in the reference's order with its separately rounded updates
+// (src/local_mover.cpp:145-204, 318-326), to compare this oracle with the
+// reference's own code (oracle/_ref) step by step.
+static int g_afterburner_reference_order = 0;
 // src/header/ordering.h:17-19
 constexpr i64 MID_CUTOFF = 64;
 constexpr i64 LARGE_CUTOFF = 128;
@@ -531,6 +537,25 @@ struct Engine {
             float multi = to_f(g.vtx_w[i]) * pm;
             float igain = gain[i];
             i32 hi = (i32)xorshift32((u32)i);
+            if (g_afterburner_reference_order) {
+                float change = 0;
+                for (i64 j = g.rowptr[i]; j < g.rowptr[i + 1]; j++) {
+                    i32 v = g.col[j];
+                    float vgain = gain[v];
+                    if ((vgain - igain) >= AFTERBURNER_EPS ||
+                        (std::fabs(vgain - igain) < AFTERBURNER_EPS && (i32)xorshift32((u32)v) < hi)) {
+                        float q = (float)g.wgt(j) - multi * to_f(g.vtx_w[v]);
+                        i32 vp = dest[v];
+                        change -= (vp == p) ? q : 0.0f;
+                        change += (vp == best && best != NEW_PART) ? q : 0.0f;
+                        vp = part[v];
+                        change += (vp == p) ? q : 0.0f;
+                        change -= (vp == best) ? q : 0.0f;
+                    }
+                }
+                keep[x] = igain + change >= 0.0f;
+                continue;
+            }
             double change = canon_vertex_sum(g.rowptr[i], g.rowptr[i + 1], [&](i64 j) -> double {
                 i32 v = g.col[j];
                 float vgain = gain[v];
@@ -712,6 +737,56 @@ struct Engine {
         i64 k = (i64)moves.size();
         std::vector<i64> prio(n, n + 1);
         for (i64 x = 0; x < k; x++) prio[moves[x]] = x;
+        if (g_afterburner_reference_order) {
+            // the reference's FP32 arithmetic in its order: per move the
+            // separately rounded updates over edges then earlier moves, an FP32
+            // inclusive scan, and the first maximum (src/local_mover.cpp:145-204)
+            std::vector<float> oc32(k);
+            for (i64 x = 0; x < k; x++) {
+                i32 i = moves[x];
+                i32 best = dest[i];
+                i32 p = part[i];
+                float w = to_f(g.vtx_w[i]);
+                float multi = w * pm;
+                float obj_change = gain[i];
+                for (i64 j = g.rowptr[i]; j < g.rowptr[i + 1]; j++) {
+                    i32 v = g.col[j];
+                    if (prio[v] < prio[i]) {
+                        const float wgt = (float)g.wgt(j);
+                        i32 vp = dest[v];
+                        obj_change -= (vp == p) ? wgt : 0.0f;
+                        obj_change += (vp == best && best != NEW_PART) ? wgt : 0.0f;
+                        vp = part[v];
+                        obj_change += (vp == p) ? wgt : 0.0f;
+                        obj_change -= (vp == best) ? wgt : 0.0f;
+                    }
+                }
+                for (i64 jx = 0; jx < x; jx++) {
+                    i32 v = moves[jx];
+                    i32 vp = dest[v];
+                    float wgt = -multi * to_f(g.vtx_w[v]);
+                    obj_change -= (vp == p) ? wgt : 0.0f;
+                    obj_change += (vp == best && best != NEW_PART) ? wgt : 0.0f;
+                    vp = part[v];
+                    obj_change += (vp == p) ? wgt : 0.0f;
+                    obj_change -= (vp == best) ? wgt : 0.0f;
+                }
+                oc32[x] = obj_change;
+            }
+            float run = 0.0f, bv32 = std::numeric_limits<float>::lowest();
+            i64 bl32 = n;
+            for (i64 x = 0; x < k; x++) {
+                run += oc32[x];
+                if (run > bv32) {
+                    bv32 = run;
+                    bl32 = x;
+                }
+            }
+            i64 truncate = 0;
+            if (bl32 < k && bv32 > 0) truncate = bl32 + 1;
+            moves.resize(truncate);
+            return;
+        }
         std::vector<double> oc(k);
         for (i64 x = 0; x < k; x++) {
             i32 i = moves[x];
@@ -1811,6 +1886,8 @@ int64_t orc_connected_components(int64_t n, const int64_t* rowptr, const int32_t
 void orc_det_scan(const double* a, double* out, int64_t k) { det_scan_incl(a, out, k); }
 double orc_det_reduce(const double* a, int64_t k) { return det_reduce(a, k); }
 uint32_t orc_murmur3(uint32_t k) { return murmur3_32(k); }
+
+void orc_set_afterburner_reference_order(int on) { g_afterburner_reference_order = on ? 1 : 0; }
 
 int orc_num_threads() {
 #ifdef _OPENMP

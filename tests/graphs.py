@@ -124,3 +124,16 @@ def symmetric_weights(hg):
     dst = hg.col.astype(np.int64)
     lo, hi = np.minimum(src, dst), np.maximum(src, dst)
     return (0.5 + ((lo * 1000003 + hi * 7919) % 1000) / 1000.0).astype(np.float32)
+
+
+def wide_int_weights(hg, hi=10000, seed=5):
+    """The same graph with symmetric int32 weights in [1, hi] from a hash of the
+    unordered pair: DeltaQ ties between clusters become vanishingly rare, so
+    tie-breaking rules stop mattering.  Totals stay far below 2^31 for the
+    test graphs (the reference sums weights in int32)."""
+    src = np.repeat(np.arange(hg.n, dtype=np.int64), np.diff(hg.rowptr))
+    dst = hg.col.astype(np.int64)
+    lo, hh = np.minimum(src, dst), np.maximum(src, dst)
+    h = (lo * 2654435761 + hh * 40503 + seed * 97) % 1000003
+    w = (1 + (h * 7919) % hi).astype(np.int32)
+    return HostGraph(hg.rowptr, hg.col, w, name=hg.name + "+wide")
