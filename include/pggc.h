@@ -362,6 +362,10 @@ pggc_status pggc_filter_log_stop(pggc_context* ctx, float* features_out, float* 
  * logit is below threshold_logit are not evaluated.  params NULL disables it.
  * The finest level's last local move of each pass always runs unfiltered. */
 pggc_status pggc_filter_enable(pggc_context* ctx, const float* params, float threshold_logit);
+/* where the enabled filter applies: sweeps of the passes before max_pass
+ * (max_pass < 0: every pass; passes count from 0 within a run_clustering) at
+ * multilevel levels >= min_level (0: the input graph).  Default: everywhere. */
+pggc_status pggc_filter_scope(pggc_context* ctx, int max_pass, int min_level);
 /* vertices evaluated / skipped by the filter since the last reset */
 pggc_status pggc_filter_stats(pggc_context* ctx, int64_t* evaluated, int64_t* skipped, int reset);
 

@@ -920,6 +920,8 @@ static void batch_impl(pggc_context* ctx, pggc_batch_job* jobs, int64_t count, i
         wc.filt.net = c.filt.net;
         wc.filt.threshold = c.filt.threshold;
         wc.filt.stats = c.filt.stats;
+        wc.filt.max_pass = c.filt.max_pass;
+        wc.filt.min_level = c.filt.min_level;
         for (;;) {
             const i64 k = next.fetch_add(1);
             if (k >= count) break;
@@ -1343,6 +1345,15 @@ pggc_status pggc_filter_enable(pggc_context* ctx, const float* params, float thr
         F.threshold = threshold_logit;
         F.mode = 2;
         c.sync();
+    });
+}
+
+pggc_status pggc_filter_scope(pggc_context* ctx, int max_pass, int min_level) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL argument");
+        need(min_level >= 0, "min_level must be >= 0");
+        ctx->ctx->filt.max_pass = max_pass < 0 ? -1 : max_pass;
+        ctx->ctx->filt.min_level = min_level;
     });
 }
 

@@ -75,6 +75,11 @@ struct Context {
         float* params = nullptr;                // FP32 master copy (device)
         float threshold = 0.f;                  // logit below which a vertex is skipped
         bool suspended = false;                 // set by the driver around exact sweeps
+        // scope: the filter gates sweeps of passes below max_pass (< 0: every
+        // pass) at levels at or above min_level; `pass` is set by the driver
+        int max_pass = -1;
+        int min_level = 0;
+        int pass = 0;
         float* log_x = nullptr;                 // [log_cap][8]
         float* log_y = nullptr;                 // [log_cap]
         i32* log_v = nullptr;                   // [log_cap]

@@ -365,6 +365,7 @@ void run_clustering(Context& ctx, const Graph<W>& g, ClusterState<typename Trait
     u64 pass = 0;
     auto one = [&](bool improve) {
         ProfScope ps(ctx, improve ? "pass_improve" : "pass_first");
+        ctx.filt.pass = (int)std::min<u64>(acc.passes, 1u << 30);
         RunStats r1;
         if (method == METHOD_LOUVAIN) {
             louvain_part<W>(ctx, g, cs, improve, con.p, part.p, &r1);

@@ -1760,7 +1760,8 @@ struct Mover {
         if (!filt_on) return;
         auto& F = ctx.filt;
         F.stamp++;
-        if (F.mode == 2 && F.suspended) return;
+        if (F.mode == 2 && (F.suspended || F.level < F.min_level || (F.max_pass >= 0 && F.pass >= F.max_pass)))
+            return;
         ProfScope ps(ctx, "filter");
         FiltArgs<W> a;
         a.g = g.view();

@@ -114,6 +114,12 @@ def disable(mem):
     check(L.lib().pggc_filter_enable(mem.handle, None, 0.0))
 
 
+def scope(mem, max_pass: int = -1, min_level: int = 0):
+    """Restrict the filter to passes before max_pass (< 0: all) and levels at
+    or above min_level."""
+    check(L.lib().pggc_filter_scope(mem.handle, int(max_pass), int(min_level)))
+
+
 def stats(mem, reset: bool = False):
     """(vertices evaluated, vertices skipped) by the filter."""
     e, s = ctypes.c_int64(), ctypes.c_int64()
