@@ -355,6 +355,10 @@ pggc_status pggc_mlp_train(pggc_context* ctx, float* params_io, const float* fea
  * each evaluated vertex is sampled with probability sample_rate, up to
  * `capacity` rows */
 pggc_status pggc_filter_log_start(pggc_context* ctx, int64_t capacity, double sample_rate, uint64_t seed);
+/* the label logged samples get: 0 (default) 1 when the vertex moves in the
+ * sweep; 1 when the sweep's select step proposes a move for it (it becomes a
+ * candidate of the afterburner) */
+pggc_status pggc_filter_log_label(pggc_context* ctx, int label);
 /* stop logging and copy out min(rows, capacity) rows; *count_out = rows logged */
 pggc_status pggc_filter_log_stop(pggc_context* ctx, float* features_out, float* labels_out, int64_t capacity,
                                  int mem_kind, int64_t* count_out);

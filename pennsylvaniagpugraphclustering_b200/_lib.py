@@ -111,6 +111,7 @@ _SIGS = {
     "pggc_filter_enable": (_ci, [_vp, _vp, _flt]),
     "pggc_filter_stats": (_ci, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), _ci]),
     "pggc_filter_scope": (_ci, [_vp, _ci, _ci]),
+    "pggc_filter_log_label": (_ci, [_vp, _ci]),
     "pggc_batch_run": (_ci, [_vp, _vp, _i64, _ci]),
     "pggc_tune_set": (_ci, [_vp, ctypes.POINTER(Tune)]),
     "pggc_tune_get": (_ci, [_vp, ctypes.POINTER(Tune)]),

@@ -1348,6 +1348,14 @@ pggc_status pggc_filter_enable(pggc_context* ctx, const float* params, float thr
     });
 }
 
+pggc_status pggc_filter_log_label(pggc_context* ctx, int label) {
+    return guarded([&] {
+        need(ctx != nullptr, "NULL argument");
+        need(label == 0 || label == 1, "label must be 0 (moved) or 1 (candidate)");
+        ctx->ctx->filt.log_label = label;
+    });
+}
+
 pggc_status pggc_filter_scope(pggc_context* ctx, int max_pass, int min_level) {
     return guarded([&] {
         need(ctx != nullptr, "NULL argument");

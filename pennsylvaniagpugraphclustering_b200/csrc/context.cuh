@@ -86,6 +86,7 @@ struct Context {
         unsigned long long* log_cnt = nullptr;  // [0] rows written, [1] first row of the current sweep
         i64 log_cap = 0;
         u32 log_rate = 0;                       // a row is sampled when its hash is below this
+        int log_label = 0;                      // 0: moved, 1: candidate (select proposed a move)
         u64 log_seed = 0;
         unsigned long long* stats = nullptr;    // [0] vertices evaluated, [1] skipped
         int level = 0;                          // current level, set by the multilevel driver

@@ -879,12 +879,12 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     }
     phase.reset();
     // algorithmic bytes: per fine edge its column, weight, the map of its head
-    // and one table insert (key + value); per fine vertex its offset and map;
-    // the coarse CSR written once
+    // and one table insert (key + output weight); per fine vertex its offset
+    // and map; the coarse CSR written once
     {
         const double wb = g.uniform ? 0.0 : (double)sizeof(W);
-        const double vb = (double)sizeof(V);
-        ctx.prof_add_bytes("contract", (double)g.nnz * (4.0 + wb + 4.0 + 4.0 + vb) + (double)g.n * (8.0 + 4.0) +
+        const double wout = (double)sizeof(W);
+        ctx.prof_add_bytes("contract", (double)g.nnz * (4.0 + wb + 4.0 + 4.0 + wout) + (double)g.n * (8.0 + 4.0) +
                                            (double)nnz_c * (4.0 + sizeof(W)) + (double)(nc + 1) * 8.0);
     }
     return cg;

@@ -12,7 +12,7 @@
 //   f7 sweep index / 8
 // In logging mode a hashed sample of those rows is appended to a log, and the
 // rows are labelled after the afterburner (1 = the vertex moves in this
-// sweep).  In filtering mode the network (mlp.cuh) scores all 32 vertices of a
+// sweep, or with the candidate label 1 = the select step proposed a move).  In filtering mode the network (mlp.cuh) scores all 32 vertices of a
 // warp on the tensor cores and the vertices whose logit is below the threshold
 // are not evaluated: their dest becomes NO_MOVE (as if evaluated without a
 // move), so they return to the sweep when a neighbour moves.  Gains of the
@@ -122,17 +122,18 @@ __global__ void __launch_bounds__(FW_WARPS * 32) k_filter_sweep(FiltArgs<W> a) {
     }
 }
 
-// labels of this sweep's samples [log_cnt[1], log_cnt[0]): 1 if the vertex
-// was a candidate the afterburner kept
+// labels of this sweep's samples [log_cnt[1], log_cnt[0]): mode 0, 1 if the
+// vertex was a candidate the afterburner kept (it moves); mode 1, 1 if the
+// select step proposed a move for it (it is a candidate)
 __global__ void k_filter_label(const i32* log_v, float* log_y, const unsigned long long* log_cnt, i64 log_cap,
-                               const i32* dest, const unsigned char* keep) {
+                               const i32* dest, const unsigned char* keep, int mode) {
     const unsigned long long lo = log_cnt[1];
     unsigned long long hi = log_cnt[0];
     if (hi > (unsigned long long)log_cap) hi = (unsigned long long)log_cap;
     for (unsigned long long r = lo + blockIdx.x * (u64)blockDim.x + threadIdx.x; r < hi;
          r += (u64)gridDim.x * blockDim.x) {
         const i32 v = log_v[r];
-        log_y[r] = (dest[v] != NO_MOVE && keep[v]) ? 1.f : 0.f;
+        log_y[r] = (dest[v] != NO_MOVE && (mode == 1 || keep[v])) ? 1.f : 0.f;
     }
 }
 

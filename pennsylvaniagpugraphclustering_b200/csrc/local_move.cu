@@ -1800,7 +1800,8 @@ struct Mover {
     void filter_post() {
         if (!filt_on || ctx.filt.mode != 1) return;
         auto& F = ctx.filt;
-        k_filter_label<<<ctx.num_sms, 256, 0, ctx.stream>>>(F.log_v, F.log_y, F.log_cnt, F.log_cap, dest.p, keep.p);
+        k_filter_label<<<ctx.num_sms, 256, 0, ctx.stream>>>(F.log_v, F.log_y, F.log_cnt, F.log_cap, dest.p, keep.p,
+                                                             F.log_label);
         PGGC_LAUNCH_CHECK();
     }
 

@@ -83,6 +83,12 @@ def log_start(mem, capacity: int, sample_rate: float = 1.0, seed: int = 1):
     check(L.lib().pggc_filter_log_start(mem.handle, int(capacity), float(sample_rate), int(seed)))
 
 
+def log_label(mem, label: str = "moved"):
+    """What logged samples are labelled with: "moved" (the vertex moves in the
+    sweep) or "candidate" (the select step proposes a move for it)."""
+    check(L.lib().pggc_filter_log_label(mem.handle, {"moved": 0, "candidate": 1}[label]))
+
+
 def log_stop(mem, capacity: int):
     """Stop logging; returns (features [k, 8], labels [k], rows logged)."""
     x = np.empty((capacity, N_FEATURES), np.float32)
