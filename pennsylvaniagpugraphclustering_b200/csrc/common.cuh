@@ -45,7 +45,7 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int NUM_SMS = 148;
 
 // device-side error codes latched in Context::d_err
-enum DevErr : int { DEV_OK = 0, DEV_ERR_PROBE = 1, DEV_ERR_CHASE = 2, DEV_ERR_LABEL = 3 };
+enum DevErr : int { DEV_OK = 0, DEV_ERR_PROBE = 1, DEV_ERR_CHASE = 2, DEV_ERR_LABEL = 3, DEV_ERR_WAIT = 4 };
 
 struct CudaError : std::runtime_error {
     cudaError_t code;

@@ -710,6 +710,188 @@ __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg
     if (a.prof && threadIdx.x == 0 && pb) atomicAdd(a.prof, pb);
 }
 
+// ---- vertices whose distinct neighbour clusters overflow a 16384-slot shared
+// table: the row is split across blocks ------------------------------------------
+// Four launches per round of up to `count` such vertices, each vertex owning a
+// global table of `gcap` slots: clear the tables; insert, one block per chunk of
+// SPLIT_CHUNK edges (the chunk's columns and weights staged in shared memory by
+// a TMA bulk copy, cp.async.bulk, from this GPU's own memory); scan, blocks over
+// table slots with a packed 64-bit atomicMax of (gain, ~cluster) per vertex --
+// the (larger gain, then smaller id) order of `better`; finish, one thread per
+// vertex.  Sums are the exact table sums of the single-block pass, so the
+// result is the same.
+constexpr int SPLIT_CHUNK = 8192;
+constexpr int SPLIT_THREADS = 256;
+constexpr size_t SPLIT_SMEM = 16 + 2 * sizeof(i32) * (SPLIT_CHUNK + 4);
+// bounded waits on the bulk copy's mbarrier (far above any copy's duration)
+constexpr u32 SPLIT_WAIT_LIMIT = 1u << 24;
+
+__device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// non-multicast bulk copy global -> this CTA's shared memory; both addresses
+// 16-byte aligned and bytes a multiple of 16 (the caller's job)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, u32 bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, u32 parity) {
+    u32 ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long pack_best(const Best& b) {
+    return ((unsigned long long)f2ord(b.jc) << 32) | (unsigned long long)(~(u32)b.c);
+}
+__device__ __forceinline__ Best unpack_best(unsigned long long k) {
+    return Best{ord2f((u32)(k >> 32)), (i32)(~(u32)(k & 0xFFFFFFFFull))};
+}
+
+template <class W>
+__global__ void k_split_clear(SelArgs<W> a, const i32* list, i64 count, i64 gcap, i32* keys,
+                              typename Traits<W>::V* vals, unsigned long long* best) {
+    using V = typename Traits<W>::V;
+    const i64 total = count * gcap;
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < total; x += (i64)gridDim.x * blockDim.x) {
+        keys[x] = -1;
+        vals[x] = V(0);
+    }
+    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < count; k += (i64)gridDim.x * blockDim.x) best[k] = 0;
+}
+
+template <class W>
+__global__ void __launch_bounds__(SPLIT_THREADS) k_split_insert(SelArgs<W> a, const i32* list, i64 count, i64 gcap,
+                                                               i32* gkeys, typename Traits<W>::V* gvals) {
+    using V = typename Traits<W>::V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned long long* bar = (unsigned long long*)smem_raw;
+    i32* s_col = (i32*)(smem_raw + 16);
+    W* s_w = (W*)(smem_raw + 16 + sizeof(i32) * (SPLIT_CHUNK + 4));
+    const i64 k = blockIdx.y;
+    if (k >= count) return;
+    const i32 i = list[k];
+    const i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+    const i64 j0 = b + (i64)blockIdx.x * SPLIT_CHUNK;
+    if (j0 >= e) return;
+    const i64 j1 = min(e, j0 + (i64)SPLIT_CHUNK);
+    const VCtx vc = sel_prologue(a, i);
+    if (sel_no_candidate(a, i, vc)) return;
+    const i64 U = min(e - b, *a.label_count);
+    u32 T = sel_table_slots(a, U);
+    if (T > (u32)gcap) T = (u32)gcap;
+    i32* keys = gkeys + k * gcap;
+    V* vals = gvals + k * gcap;
+    // stage [j0, j1): the 16-byte-aligned middle by bulk copy, the ragged
+    // tail by plain loads (the head below j0 is copied and ignored)
+    const bool has_w = a.g.w != nullptr;
+    const i64 lo16 = j0 & ~(i64)3, hi16 = j1 & ~(i64)3;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(a.g.col) & 15) == 0) &&
+                         (!has_w || (reinterpret_cast<uintptr_t>(a.g.w) & 15) == 0);
+    const u32 bytes = (aligned && hi16 > lo16) ? (u32)((hi16 - lo16) * 4) : 0u;
+    if (threadIdx.x == 0 && bytes) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && bytes) {
+        mbar_expect_tx(bar, has_w ? 2 * bytes : bytes);
+        bulk_g2s(s_col, a.g.col + lo16, bytes, bar);
+        if (has_w) bulk_g2s(s_w, a.g.w + lo16, bytes, bar);
+    }
+    const i64 plain_from = bytes ? max(hi16, j0) : j0;
+    for (i64 j = plain_from + threadIdx.x; j < j1; j += SPLIT_THREADS) {
+        s_col[j - lo16] = a.g.col[j];
+        if (has_w) s_w[j - lo16] = a.g.w[j];
+    }
+    // one thread waits (bounded) for the bulk copy and tells the block
+    __shared__ int staged;
+    if (threadIdx.x == 0) {
+        bool done = bytes == 0;
+        for (u32 it = 0; it < SPLIT_WAIT_LIMIT && !done; it++) done = mbar_try_wait(bar, 0);
+        if (!done) {
+            // never expected: report, wait (bounded) for the copy that still
+            // targets this block's shared memory, and give up the chunk
+            atomicExch(a.err, (int)DEV_ERR_WAIT);
+            for (u32 it = 0; it < SPLIT_WAIT_LIMIT && !done; it++) done = mbar_try_wait(bar, 0);
+        }
+        staged = done ? 1 : 0;
+    }
+    __syncthreads();
+    if (!staged) return;
+    const int l = lane_id(), w = threadIdx.x >> 5;
+    const i64 len = j1 - j0, base = j0 - lo16;
+    for (i64 t = (i64)w * 32 + l; t - l < len; t += SPLIT_THREADS) {
+        const bool valid = t < len;
+        const i32 c = valid ? a.part[s_col[base + t]] : -1;
+        const W wr = valid ? (has_w ? s_w[base + t] : W(1)) : W(0);
+        const bool keep = valid && c != vc.p;
+        const i32 key = keep ? c : (i32)(0x80000000u | l);
+        const unsigned peers = __match_any_sync(FULL, key);
+        const bool leader = keep && ((peers & lanemask_lt()) == 0);
+        const V sum = peer_sum<W>(a, peers, wr, keep, leader);
+        if (leader) table_add(keys, vals, T - 1, c, sum, a.err, a.probe_cap);
+    }
+}
+
+template <class W, bool CON>
+__global__ void __launch_bounds__(SPLIT_THREADS) k_split_scan(SelArgs<W> a, const i32* list, i64 count, i64 gcap,
+                                                             const i32* gkeys, const typename Traits<W>::V* gvals,
+                                                             unsigned long long* best) {
+    __shared__ Best wb[SPLIT_THREADS / 32];
+    const i64 k = blockIdx.y;
+    if (k >= count) return;
+    const i32 i = list[k];
+    const i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+    const VCtx vc = sel_prologue(a, i);
+    if (sel_no_candidate(a, i, vc)) return;
+    const i64 U = min(e - b, *a.label_count);
+    u32 T = sel_table_slots(a, U);
+    if (T > (u32)gcap) T = (u32)gcap;
+    const i32* keys = gkeys + k * gcap;
+    const auto* vals = gvals + k * gcap;
+    Best bst = none_best();
+    for (i64 sl = blockIdx.x * (i64)SPLIT_THREADS + threadIdx.x; sl < T; sl += (i64)gridDim.x * SPLIT_THREADS) {
+        const i32 c = keys[sl];
+        if (c != -1) sel_eval<W, CON>(a, vc, c, vals[sl], bst);
+    }
+    warp_best(bst);
+    const int l = lane_id(), w = threadIdx.x >> 5;
+    if (l == 0) wb[w] = bst;
+    __syncthreads();
+    if (w == 0) {
+        bst = l < SPLIT_THREADS / 32 ? wb[l] : none_best();
+        warp_best(bst);
+        if (l == 0 && bst.c != 2147483647) atomicMax(&best[k], pack_best(bst));
+    }
+}
+
+template <class W>
+__global__ void k_split_finish(SelArgs<W> a, const i32* list, i64 count, const unsigned long long* best) {
+    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < count; k += (i64)gridDim.x * blockDim.x) {
+        const i32 i = list[k];
+        const VCtx vc = sel_prologue(a, i);
+        const bool none = sel_no_candidate(a, i, vc) || best[k] == 0;
+        const Best bst = none ? none_best() : unpack_best(best[k]);
+        sel_finish(a, i, vc, bst);
+        if (a.prof) {
+            const i64 deg = none && sel_no_candidate(a, i, vc) ? 0 : a.g.rowptr[i + 1] - a.g.rowptr[i];
+            atomicAdd(a.prof, sel_bytes(a, deg, true));
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // own-cluster weights (pvals)
 // ---------------------------------------------------------------------------
@@ -1702,7 +1884,7 @@ struct Mover {
 
     enum Slot { S_PART, S_DEST, S_CAND, S_MOVES, S_NEWL, S_AVAIL, S_PRIO, S_GAIN, S_PV, S_PVC, S_TD, S_FLAGS, S_KEEP,
                 S_HAS, S_SC, S_GK, S_GV, S_CLS, S_CLS_OFF, S_CLS_CNT, S_MOVED_AT, S_CSIZE, S_OVF, S_OVF_CNT,
-                S_STAMP, S_AFF, S_AFF_CNT };
+                S_STAMP, S_AFF, S_AFF_CNT, S_SPLIT_BEST };
 
     Mover(Context& c, const Graph<W>& gr, const Ordering& o, i64 capacity)
         : ctx(c), g(gr), ord(o), n(gr.n), cap(capacity) {
@@ -1905,9 +2087,29 @@ struct Mover {
             k_select_block<W, CON, false, 1024, true><<<grid, 1024, slot * TS, ctx.stream>>>(
                 ah, host_range(ord.huge.p, 0, ord.n_huge), nullptr, nullptr, TS, ovf, ovf_cnt);
             PGGC_LAUNCH_CHECK();
-            k_select_block<W, CON, true><<<gblocks, 256, 0, ctx.stream>>>(a, Range{ovf, nullptr, ovf_cnt, 0, 0}, gkeys.p,
-                                                                        gvals.p, gcap);
-            PGGC_LAUNCH_CHECK();
+            // the vertices that overflowed: rows split across blocks, in rounds
+            // of up to gblocks vertices (one table each)
+            const i64 n_ovf = ctx.read1(ovf_cnt);
+            unsigned long long* sbest = ctx.ws_get<unsigned long long>(S_SPLIT_BEST, gblocks);
+            set_dynamic_smem_once(k_split_insert<W>, (int)SPLIT_SMEM, ctx.device);
+            const unsigned chunks = (unsigned)std::max<i64>(1, ceil_div(ord.max_deg, SPLIT_CHUNK));
+            for (i64 r0 = 0; r0 < n_ovf; r0 += gblocks) {
+                const i64 cnt = std::min<i64>(gblocks, n_ovf - r0);
+                const i32* lst = ovf + r0;
+                const int cgrid = grid_for(ctx, cnt * gcap, 256, 16);
+                k_split_clear<W><<<cgrid, 256, 0, ctx.stream>>>(a, lst, cnt, gcap, gkeys.p, gvals.p, sbest);
+                PGGC_LAUNCH_CHECK();
+                k_split_insert<W><<<dim3(chunks, (unsigned)cnt), SPLIT_THREADS, SPLIT_SMEM, ctx.stream>>>(
+                    a, lst, cnt, gcap, gkeys.p, gvals.p);
+                PGGC_LAUNCH_CHECK();
+                const unsigned sblocks =
+                    (unsigned)std::max<i64>(1, std::min<i64>(ceil_div(gcap, SPLIT_THREADS * 8), (i64)ctx.num_sms));
+                k_split_scan<W, CON><<<dim3(sblocks, (unsigned)cnt), SPLIT_THREADS, 0, ctx.stream>>>(
+                    a, lst, cnt, gcap, gkeys.p, gvals.p, sbest);
+                PGGC_LAUNCH_CHECK();
+                k_split_finish<W><<<1, 256, 0, ctx.stream>>>(a, lst, cnt, sbest);
+                PGGC_LAUNCH_CHECK();
+            }
         }
     }
     void launch_select(const SelArgs<W>& a, bool constrained) {

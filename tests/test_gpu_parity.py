@@ -351,3 +351,36 @@ def test_build_coarse_graph_above_bitmap_limit(mem, weighted):
         assert np.array_equal(col_o, col_g)
         assert np.array_equal(w_o, w_g)
         assert np.array_equal(vw_o, vw_g)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("fr", [0.0, 0.75])
+def test_select_pass_hub_row_at_unaligned_offset(mem, weighted, fr):
+    """A 40,000-leaf hub whose row starts 6 edges into the column array (not on
+    a 16-byte boundary) and ends on a ragged tail: the split select stages
+    each 8192-edge chunk with a bulk copy of its aligned middle and plain loads
+    of the rest; the result must equal the oracle's."""
+    leaves = 40000
+    edges = [(0, 1), (1, 2), (0, 2)] + [(3, 4 + k) for k in range(leaves)]
+    rng = np.random.default_rng(21)
+    w = rng.uniform(0.5, 1.5, len(edges)).astype(np.float32) if weighted else None
+    hg = G.from_edges(4 + leaves, edges, w)
+    assert hg.rowptr[3] % 4 != 0 and hg.rowptr[4] % 4 != 0
+    obj = pg.OBJ_WMOD if weighted else pg.OBJ_MOD
+    og, wg = _pair(mem, hg, obj)
+    n = hg.n
+    cd_o = O.ClusterData(og, obj, 1.0)
+    cd_g = pg.get_objective(mem, wg, obj, 1.0)
+    part = np.arange(n, dtype=np.int32)
+    _, _, _, vw = og.arrays()
+    td = vw.astype(wg.vdtype)
+    pv = np.zeros(n, wg.vdtype)
+    cd_o.set_state(td, 0)
+    cd_g.set_state(n, td, 0)
+    dest0 = np.full(n, pg.NULL_PART, np.int32)
+    gain0 = np.zeros(n, np.float32)
+    do, go, ko = O.select(og, cd_o, part, pv, dest0, fr, False, gain=gain0)
+    dg, gg_, kg = pg.select_pass(mem, wg, cd_g, part, pv, dest0, fr, False, gain=gain0)
+    assert ko == kg
+    assert np.array_equal(do, dg)
+    assert np.array_equal(go.view(np.int32), gg_.view(np.int32))
