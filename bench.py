@@ -24,9 +24,12 @@ time (the reference's "Cluster time" span), at equal modularity:
 * ``e2e``: a batch of P members through the public C ABI from host buffers:
   CSR upload, graph + objective construction, clustering and label download.
 
-The filter is trained before the warm-up (untimed) on move labels logged from
-plain first passes of the three named workloads' generators at seeds 1-8:
-planted SBM n = 65,536, the DC-SBM at n = 262,144, R-MAT scale 18.
+The filter is trained before the warm-up (untimed) on move / no-move labels
+logged from plain first passes of the three named workloads' generators at
+seeds 1-8 (planted SBM n = 65,536, the DC-SBM at n = 262,144, R-MAT scale 18):
+by default the label is the select step's decision (it proposes a move or
+not), the threshold keeps 99.5 % of the proposals, and the filter gates the
+sweeps of the coarse levels (>= 1), where they are latency-bound.
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (the reference itself needs Kokkos, which is unavailable) on a bounded sample of
@@ -73,12 +76,16 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4194304, help="DC-SBM vertex count (default: the named workload)")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--streams", type=int, default=4, help="worker streams of the batch (population width)")
+    ap.add_argument("--streams", type=int, default=6, help="worker streams of the batch (population width)")
     ap.add_argument("--plain-runs", type=int, default=2,
                     help="plain runs (the first seeds of the population, no filter, one stream) for the ratio")
     ap.add_argument("--no-filter", action="store_true", help="batched plain runs (no learned filter)")
-    ap.add_argument("--recall", type=float, default=0.98,
+    ap.add_argument("--recall", type=float, default=0.995,
                     help="recall on the training logs that sets the filter's logit threshold")
+    ap.add_argument("--filter-label", default="candidate", choices=["candidate", "moved"],
+                    help="training label: the select step proposes a move (candidate) or the vertex moves")
+    ap.add_argument("--filter-min-level", type=int, default=1,
+                    help="the filter gates sweeps at multilevel levels >= this (0: the input graph too)")
     ap.add_argument("--cpu-sample-n", type=int, default=262144)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None, help="e2e batch size (default: --streams)")
@@ -222,15 +229,17 @@ def traffic_for(family):
 
 
 
-def train_filter(pg, mem, recall):
-    """Train the learned move filter on move labels logged from plain first
-    passes of the named workloads' generators at seeds 1-8 (planted SBM
-    n = 65,536; the DC-SBM at n = 262,144; R-MAT scale 18); returns
-    (params, threshold, info)."""
+def train_filter(pg, mem, recall, label="candidate"):
+    """Train the learned move filter on move / no-move labels logged from
+    plain first passes of the named workloads' generators at seeds 1-8
+    (planted SBM n = 65,536; the DC-SBM at n = 262,144; R-MAT scale 18);
+    returns (params, threshold, info).  label "candidate": 1 when the select
+    step proposes a move for the vertex; "moved": 1 when it moves."""
     from pennsylvaniagpugraphclustering_b200 import graphgen as gg, move_filter as MF
     t0 = time.perf_counter()
     xs, ys = [], []
     cap = 400_000
+    MF.log_label(mem, label)
     for s in range(1, 9):
         for kind in ("sbm", "dcsbm", "rmat"):
             if kind == "sbm":
@@ -250,13 +259,16 @@ def train_filter(pg, mem, recall):
             ys.append(y)
             cd.close()
             g2.close()
+    MF.log_label(mem, "moved")
     x = np.concatenate(xs)
     y = np.concatenate(ys)
     pos_w = float(min(20.0, (len(y) - y.sum()) / max(y.sum(), 1.0)))
     params, losses = MF.train(mem, MF.init_params(1), x, y, epochs=6, batch=4096, lr=3e-3, pos_weight=pos_w)
     thr = MF.threshold_for_recall(mem, params, x, y, recall=recall)
+    skip = float(np.mean(MF.infer(mem, params, x) < thr))
     return params, thr, {"train_rows": int(len(y)), "positive_rows": int(y.sum()), "final_loss": float(losses[-1]),
-                         "threshold_logit": thr, "recall": recall, "train_seconds": time.perf_counter() - t0,
+                         "threshold_logit": thr, "recall": recall, "label": label,
+                         "train_rows_below_threshold": skip, "train_seconds": time.perf_counter() - t0,
                          "sources": "first passes of planted SBM 65,536, DC-SBM 262,144 and R-MAT 18, seeds 1-8"}
 
 
@@ -285,7 +297,9 @@ def ours(args):
     filt_info = None
     params = thr = None
     if learned:
-        params, thr, filt_info = train_filter(pg, mem, args.recall)
+        params, thr, filt_info = train_filter(pg, mem, args.recall, args.filter_label)
+        filt_info["min_level"] = args.filter_min_level
+        MF.scope(mem, -1, args.filter_min_level)
 
     def jobs(sds, ex=args.ex_iters):
         return [dict(graph=wg, objective=pg.OBJ_WMOD, method=pg.METHOD_LEIDEN_PLUS, ex_iters=ex, seed=sd)
