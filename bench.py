@@ -93,10 +93,13 @@ def parse():
                     help="profiled run also splits each kernel family by multilevel level (adds 'by_level')")
     ap.add_argument("--ex-iters", type=int, default=-1,
                     help="pLeiden+ passes after the first (-1: until the objective stops rising)")
-    ap.add_argument("--workload", default="dcsbm4m", choices=["dcsbm4m", "rmat24", "sbm65k", "sbm-population"],
+    ap.add_argument("--workload", default="dcsbm4m",
+                    choices=["dcsbm4m", "rmat24", "sbm65k", "sbm-population", "filter-eval"],
                     help="dcsbm4m: the headline line (batched+learned vs plain pLeiden+); rmat24: plain pLouvain "
                          "on R-MAT scale 24 (contraction stress); sbm65k: plain pLouvain on the planted SBM; "
-                         "sbm-population: 256 uneven SBMs, batched (autotuned) vs sequential pLeiden+")
+                         "sbm-population: 256 uneven SBMs, batched (autotuned) vs sequential pLeiden+; "
+                         "filter-eval: the trained filter against plain pLeiden+ on unseen seed 99 graphs "
+                         "(R-MAT scale 25, DC-SBM n=16,777,216 at mu=0.5)")
     ap.add_argument("--population", type=int, default=256, help="sbm-population: number of graphs")
     ap.add_argument("--rmat-scale", type=int, default=24)
     return ap.parse_args()
@@ -238,7 +241,8 @@ def train_filter(pg, mem, recall, label="candidate"):
     from pennsylvaniagpugraphclustering_b200 import graphgen as gg, move_filter as MF
     t0 = time.perf_counter()
     xs, ys = [], []
-    cap = 400_000
+    cap = 2_000_000  # above any one run's sampled rows: a full log would keep a race-dependent subset
+    truncated = 0
     MF.log_label(mem, label)
     for s in range(1, 9):
         for kind in ("sbm", "dcsbm", "rmat"):
@@ -254,7 +258,8 @@ def train_filter(pg, mem, recall, label="candidate"):
             cd = pg.get_objective(mem, g2, obj, 1.0)
             method = pg.METHOD_LOUVAIN if kind != "dcsbm" else pg.METHOD_LEIDEN_PLUS
             pg.run_clustering(mem, g2, cd, method=method, ex_iters=0, seed=s)
-            x, y, _ = MF.log_stop(mem, cap)
+            x, y, rows = MF.log_stop(mem, cap)
+            truncated += max(0, rows - cap)
             xs.append(x)
             ys.append(y)
             cd.close()
@@ -262,12 +267,17 @@ def train_filter(pg, mem, recall, label="candidate"):
     MF.log_label(mem, "moved")
     x = np.concatenate(xs)
     y = np.concatenate(ys)
+    # the log's row order depends on which warp appended first; a canonical
+    # order (features, then label) makes the minibatches, and so the trained
+    # network and its threshold, the same on every run
+    order = np.lexsort(np.concatenate([y[None, :], x.T[::-1]], axis=0))
+    x, y = x[order], y[order]
     pos_w = float(min(20.0, (len(y) - y.sum()) / max(y.sum(), 1.0)))
     params, losses = MF.train(mem, MF.init_params(1), x, y, epochs=6, batch=4096, lr=3e-3, pos_weight=pos_w)
     thr = MF.threshold_for_recall(mem, params, x, y, recall=recall)
     skip = float(np.mean(MF.infer(mem, params, x) < thr))
     return params, thr, {"train_rows": int(len(y)), "positive_rows": int(y.sum()), "final_loss": float(losses[-1]),
-                         "threshold_logit": thr, "recall": recall, "label": label,
+                         "threshold_logit": thr, "recall": recall, "label": label, "rows_dropped": truncated,
                          "train_rows_below_threshold": skip, "train_seconds": time.perf_counter() - t0,
                          "sources": "first passes of planted SBM 65,536, DC-SBM 262,144 and R-MAT 18, seeds 1-8"}
 
@@ -704,6 +714,65 @@ def population(args):
     print(json.dumps(line), flush=True)
 
 
+def filter_eval(args):
+    """The learned filter on unseen graphs (seed 99): R-MAT scale 25 (Mod) and a
+    DC-SBM with n = 16,777,216 at mu = 0.5 (WMod, FP32 weights), pLeiden+ until
+    stable, one run plain and one with the filter (and its judge), one stream,
+    CUDA events.  The filter is trained as for the headline line."""
+    import torch
+    import pennsylvaniagpugraphclustering_b200 as pg
+    from pennsylvaniagpugraphclustering_b200 import graphgen as gg, move_filter as MF
+    torch.cuda.set_device(0)
+    mem = pg.memory_store(0)
+    stream = torch.cuda.ExternalStream(mem.stream(), device=torch.device("cuda", 0))
+    params, thr, info = train_filter(pg, mem, args.recall, args.filter_label)
+    MF.scope(mem, -1, args.filter_min_level)
+    out = {"metric": "Leiden edges/s, learned filter vs plain on unseen seed-99 graphs", "unit": UNIT,
+           "filter": dict(info, min_level=args.filter_min_level), "graphs": {}}
+    for name in ("rmat25", "dcsbm16m"):
+        t0 = time.perf_counter()
+        if name == "rmat25":
+            h = gg.rmat(25, 16, 0.57, 0.19, 0.19, 99)
+            obj, w = pg.OBJ_MOD, None
+        else:
+            h = gg.dcsbm(16777216, 99, mean_deg=gg.DCSBM_4M_MEAN_DEG, mu=0.5)
+            obj, w = pg.OBJ_WMOD, h.w
+        gen_s = time.perf_counter() - t0
+        g = pg.weighted_graph(mem, h.rowptr, h.col, w, objective=obj)
+        rec = {"n": h.n, "m_undirected": h.m, "objective": "Mod" if obj == pg.OBJ_MOD else "WMod",
+               "generator_seconds": gen_s}
+        for mode in ("plain", "learned"):
+            if mode == "learned":
+                MF.enable(mem, params, thr)
+                MF.stats(mem, reset=True)
+            try:
+                cd = pg.get_objective(mem, g, obj, 1.0)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                lab, st = pg.run_clustering(mem, g, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=-1, seed=99)
+                e1.record(stream)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                ev, sk = MF.stats(mem) if mode == "learned" else (0, 0)
+            finally:
+                if mode == "learned":
+                    MF.disable(mem)
+            q, _ = pg.verify_objective(mem, g, lab, obj)
+            rec[mode] = {"edges_per_s": h.m / (ms / 1000.0), "seconds": ms / 1000.0, "modularity": st["objective"],
+                         "verify_modularity": q, "passes": st["passes"], "filtered_passes": st["filtered_passes"],
+                         "exact_passes": st["exact_passes"], "judge_gain": st["judge_gain"],
+                         "fell_back": st["fell_back"], "filter_skipped_frac": sk / max(ev + sk, 1)}
+            cd.close()
+        rec["speedup"] = rec["learned"]["edges_per_s"] / rec["plain"]["edges_per_s"]
+        rec["modularity_delta"] = rec["learned"]["modularity"] - rec["plain"]["modularity"]
+        out["graphs"][name] = rec
+        g.close()
+        del h
+        print(json.dumps({name: rec}), file=sys.stderr, flush=True)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -712,6 +781,8 @@ def main():
         ours(args)
     elif args.workload == "sbm-population":
         population(args)
+    elif args.workload == "filter-eval":
+        filter_eval(args)
     else:
         plain_workload(args)
 

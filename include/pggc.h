@@ -289,7 +289,9 @@ typedef struct pggc_tune_trial {
  * are, repeatedly): after one warm-up batch at the current settings, batch
  * width over {1, 4, 8, 16, 32} (at most `count`), then the thread / warp
  * degree bounds over {(32,127), (16,127), (8,127), (0,127), (32,32), (8,32)},
- * then the load factor over {0.5, 0.7}, each step keeping the fastest.  The
+ * then the load factor over {0.5, 0.7}, each step keeping the fastest (a
+ * configuration's time is the better of two batches, and a challenger wins
+ * only when more than 2 % faster).  The
  * best configuration is set on the context and written to *best; the trials
  * (at most trials_cap) to `trials`, their number to *n_trials.  Job outputs
  * hold the last trial's results. */

@@ -1034,15 +1034,19 @@ pggc_status pggc_batch_autotune(pggc_context* ctx, pggc_batch_job* jobs, int64_t
         PGGC_CUDA(cudaEventCreate(&e0));
         PGGC_CUDA(cudaEventCreate(&e1));
         i64 nt = 0;
+        // a configuration's time is the better of two batches
         auto trial = [&](const TuneParams& p) -> double {
             c.tune = p;
-            PGGC_CUDA(cudaEventRecord(e0, c.stream));
-            batch_impl(ctx, jobs, count, p.streams);
-            PGGC_CUDA(cudaEventRecord(e1, c.stream));
-            PGGC_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            PGGC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            const double sec = ms / 1000.0;
+            double sec = 1e300;
+            for (int rep = 0; rep < 2; rep++) {
+                PGGC_CUDA(cudaEventRecord(e0, c.stream));
+                batch_impl(ctx, jobs, count, p.streams);
+                PGGC_CUDA(cudaEventRecord(e1, c.stream));
+                PGGC_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                PGGC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                sec = std::min(sec, ms / 1000.0);
+            }
             if (nt < trials_cap) {
                 trials[nt].config = tune_to(p);
                 trials[nt].seconds = sec;
@@ -1059,9 +1063,11 @@ pggc_status pggc_batch_autotune(pggc_context* ctx, pggc_batch_job* jobs, int64_t
             batch_impl(ctx, jobs, count, cur.streams);
             TuneParams bestp = cur;
             double best_s = 1e300;
+            // a challenger replaces the best only when more than 2 % faster,
+            // so timing noise does not move the knobs
             auto consider = [&](TuneParams p) {
                 const double sec = trial(p);
-                if (sec < best_s) {
+                if (best_s >= 1e299 || sec < 0.98 * best_s) {
                     best_s = sec;
                     bestp = p;
                 }
