@@ -22,6 +22,7 @@
 // The output is the canonical (row, col)-sorted coarse CSR.
 #include <optional>
 #include "kernels.cuh"
+#include "bulk.cuh"
 
 namespace pggc {
 
@@ -341,6 +342,105 @@ __global__ void __launch_bounds__(THREADS) k_contract_block(CArgs<W> a, const i3
         __syncthreads();
         if (threadIdx.x == 0) a.ucount[c] = (i64)wcount;
         __syncthreads();
+    }
+}
+
+// ---- coarse rows that overflow a 16384-slot shared table: the row's flat list
+// split across blocks ---------------------------------------------------------
+// Per round of up to `count` such rows, each owning a global table of `gcap`
+// slots: clear; insert, one block per chunk of CSPLIT_CHUNK flat entries (keys
+// and weights staged in shared memory by TMA bulk copies); write, blocks over
+// table slots appending the row's unique entries at q0 + (a per-row atomic
+// counter, ucount[c]).  The order inside the row's scratch range depends on
+// the blocks' race, but the placement sorts every row, so the coarse CSR is
+// the same; the sums are exact.
+constexpr int CSPLIT_CHUNK = 8192;
+constexpr int CSPLIT_THREADS = 256;
+constexpr size_t CSPLIT_SMEM = 16 + 2 * sizeof(i32) * (CSPLIT_CHUNK + 4);
+
+template <class W>
+__global__ void k_csplit_clear(CArgs<W> a, const i32* list, i64 count, i64 gcap, i32* keys,
+                               typename Traits<W>::V* vals) {
+    using V = typename Traits<W>::V;
+    const i64 total = count * gcap;
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < total; x += (i64)gridDim.x * blockDim.x) {
+        keys[x] = -1;
+        vals[x] = V(0);
+    }
+    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < count; k += (i64)gridDim.x * blockDim.x)
+        a.ucount[list[k]] = 0;
+}
+
+template <class W>
+__device__ __forceinline__ u32 csplit_slots(const CArgs<W>& a, i32 c, i64 nc, i64 gcap, i64& q0, i64& q1) {
+    q0 = a.P[a.cstart[c]];
+    q1 = a.P[a.cstart[c + 1]];
+    const i64 U = min(q1 - q0, nc);
+    u32 T = next_pow2_u32((u32)(2 * (U > 1 ? U : 1)));
+    return T > (u32)gcap ? (u32)gcap : T;
+}
+
+template <class W>
+__global__ void __launch_bounds__(CSPLIT_THREADS) k_csplit_insert(CArgs<W> a, const i32* list, i64 count, i64 gcap,
+                                                                 i32* gkeys, typename Traits<W>::V* gvals, i64 nc) {
+    using V = typename Traits<W>::V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned long long* bar = (unsigned long long*)smem_raw;
+    i32* s_key = (i32*)(smem_raw + 16);
+    W* s_w = (W*)(smem_raw + 16 + sizeof(i32) * (CSPLIT_CHUNK + 4));
+    const i64 k = blockIdx.y;
+    if (k >= count) return;
+    const i32 c = list[k];
+    i64 q0, q1;
+    const u32 T = csplit_slots(a, c, nc, gcap, q0, q1);
+    const i64 j0 = q0 + (i64)blockIdx.x * CSPLIT_CHUNK;
+    if (j0 >= q1) return;
+    const i64 j1 = min(q1, j0 + (i64)CSPLIT_CHUNK);
+    const bool has_w = a.g.w != nullptr;
+    if (!stage_rows(a.fkey, has_w ? a.fw : (const W*)nullptr, j0, j1, s_key, s_w, bar, a.err)) return;
+    i32* keys = gkeys + k * gcap;
+    V* vals = gvals + k * gcap;
+    const int l = lane_id(), w = threadIdx.x >> 5;
+    const i64 len = j1 - j0, base = j0 - (j0 & ~(i64)3);
+    for (i64 t = (i64)w * 32 + l; t - l < len; t += CSPLIT_THREADS) {
+        const bool valid = t < len;
+        const i32 u = valid ? s_key[base + t] : -1;
+        const V wv = (valid && has_w) ? V(s_w[base + t]) : V(0);
+        const bool keep = valid && u >= 0;
+        const i32 key = keep ? u : (i32)(0x80000000u | l);
+        const unsigned peers = __match_any_sync(FULL, key);
+        const bool leader = keep && ((peers & lanemask_lt()) == 0);
+        const V sum = has_w ? cgroup_sum<V>(peers, wv, leader) : V(__popc(peers));
+        if (leader) ctable_add(keys, vals, T - 1, key, sum, a.err, a.probe_cap);
+    }
+}
+
+template <class W>
+__global__ void __launch_bounds__(CSPLIT_THREADS) k_csplit_write(CArgs<W> a, const i32* list, i64 count, i64 gcap,
+                                                                const i32* gkeys,
+                                                                const typename Traits<W>::V* gvals, i64 nc) {
+    const i64 k = blockIdx.y;
+    if (k >= count) return;
+    const i32 c = list[k];
+    i64 q0, q1;
+    const u32 T = csplit_slots(a, c, nc, gcap, q0, q1);
+    const i32* keys = gkeys + k * gcap;
+    const auto* vals = gvals + k * gcap;
+    const int l = lane_id();
+    for (i64 s0 = blockIdx.x * (i64)CSPLIT_THREADS + (threadIdx.x & ~31); s0 < T;
+         s0 += (i64)gridDim.x * CSPLIT_THREADS) {
+        const i64 sl = s0 + l;
+        const bool occ = sl < T && keys[sl] != -1;
+        const unsigned m = __ballot_sync(FULL, occ);
+        if (!m) continue;
+        unsigned long long basepos = 0;
+        if (l == 0) basepos = ::atomicAdd((unsigned long long*)&a.ucount[c], (unsigned long long)__popc(m));
+        basepos = __shfl_sync(FULL, basepos, 0);
+        if (occ) {
+            const i64 pos = q0 + (i64)basepos + __popc(m & lanemask_lt());
+            a.out_key[pos] = keys[sl];
+            a.out_val[pos] = vals[sl];
+        }
     }
 }
 
@@ -786,14 +886,32 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
         // tables (allocated only when some row overflowed)
         const i64 n_ovf = ctx.read1(counts.p + 6);
         if (n_ovf > 0) {
+            // split across blocks, in rounds of up to `per` rows (one table
+            // each, at most 2 GiB of tables)
             i64 maxb = std::min<i64>(max_huge, nc);
             i64 gcap = next_pow2_u32((u32)std::min<i64>(2 * std::max<i64>(maxb, 1), (i64)1 << 30));
             i64 by_mem = std::max<i64>(1, ((i64)2 << 30) / (gcap * (i64)slot));
-            int ggrid = (int)std::min<i64>(std::min<i64>(n_ovf, (i64)ctx.num_sms * 2), by_mem);
-            i32* gk = ctx.ws_get<i32>(WS_CONTRACT_GK, gcap * ggrid);
-            V* gvv = ctx.ws_get<V>(WS_CONTRACT_GV, gcap * ggrid);
-            k_contract_block<W, true><<<ggrid, 256, 0, ctx.stream>>>(a, lo.p, counts.p + 6, gk, gvv, gcap, nc);
-            PGGC_LAUNCH_CHECK();
+            const i64 per = std::min<i64>(std::min<i64>(n_ovf, 32), by_mem);
+            i32* gk = ctx.ws_get<i32>(WS_CONTRACT_GK, gcap * per);
+            V* gvv = ctx.ws_get<V>(WS_CONTRACT_GV, gcap * per);
+            set_dynamic_smem_once(k_csplit_insert<W>, (int)CSPLIT_SMEM, ctx.device);
+            const unsigned chunks = (unsigned)std::max<i64>(1, ceil_div(max_huge, CSPLIT_CHUNK));
+            const unsigned wblocks =
+                (unsigned)std::max<i64>(1, std::min<i64>(ceil_div(gcap, CSPLIT_THREADS * 8), (i64)ctx.num_sms));
+            for (i64 r0 = 0; r0 < n_ovf; r0 += per) {
+                const i64 cnt = std::min<i64>(per, n_ovf - r0);
+                const i32* lst = lo.p + r0;
+                const int cgrid = (int)std::max<i64>(1, std::min<i64>(ceil_div(cnt * gcap, 256),
+                                                                      (i64)ctx.num_sms * 16));
+                k_csplit_clear<W><<<cgrid, 256, 0, ctx.stream>>>(a, lst, cnt, gcap, gk, gvv);
+                PGGC_LAUNCH_CHECK();
+                k_csplit_insert<W><<<dim3(chunks, (unsigned)cnt), CSPLIT_THREADS, CSPLIT_SMEM, ctx.stream>>>(
+                    a, lst, cnt, gcap, gk, gvv, nc);
+                PGGC_LAUNCH_CHECK();
+                k_csplit_write<W><<<dim3(wblocks, (unsigned)cnt), CSPLIT_THREADS, 0, ctx.stream>>>(a, lst, cnt, gcap,
+                                                                                                    gk, gvv, nc);
+                PGGC_LAUNCH_CHECK();
+            }
         }
     }
     // coarse row offsets, placement buckets and the big-row total, then one round trip

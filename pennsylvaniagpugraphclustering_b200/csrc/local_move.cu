@@ -19,6 +19,7 @@
 //    reads counts from device memory.
 #include <mutex>
 #include "kernels.cuh"
+#include "bulk.cuh"
 #include "filter.cuh"
 
 namespace pggc {
@@ -723,35 +724,6 @@ __global__ void __launch_bounds__(THREADS) k_select_block(SelArgs<W> a, Range rg
 constexpr int SPLIT_CHUNK = 8192;
 constexpr int SPLIT_THREADS = 256;
 constexpr size_t SPLIT_SMEM = 16 + 2 * sizeof(i32) * (SPLIT_CHUNK + 4);
-// bounded waits on the bulk copy's mbarrier (far above any copy's duration)
-constexpr u32 SPLIT_WAIT_LIMIT = 1u << 24;
-
-__device__ __forceinline__ u32 smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, u32 count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, u32 bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// non-multicast bulk copy global -> this CTA's shared memory; both addresses
-// 16-byte aligned and bytes a multiple of 16 (the caller's job)
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, u32 bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, u32 parity) {
-    u32 ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
 __device__ __forceinline__ unsigned long long pack_best(const Best& b) {
     return ((unsigned long long)f2ord(b.jc) << 32) | (unsigned long long)(~(u32)b.c);
 }
@@ -793,43 +765,10 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_insert(SelArgs<W> a, co
     if (T > (u32)gcap) T = (u32)gcap;
     i32* keys = gkeys + k * gcap;
     V* vals = gvals + k * gcap;
-    // stage [j0, j1): the 16-byte-aligned middle by bulk copy, the ragged
-    // tail by plain loads (the head below j0 is copied and ignored)
+    // stage the chunk's columns (and weights) in shared memory
     const bool has_w = a.g.w != nullptr;
-    const i64 lo16 = j0 & ~(i64)3, hi16 = j1 & ~(i64)3;
-    const bool aligned = ((reinterpret_cast<uintptr_t>(a.g.col) & 15) == 0) &&
-                         (!has_w || (reinterpret_cast<uintptr_t>(a.g.w) & 15) == 0);
-    const u32 bytes = (aligned && hi16 > lo16) ? (u32)((hi16 - lo16) * 4) : 0u;
-    if (threadIdx.x == 0 && bytes) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && bytes) {
-        mbar_expect_tx(bar, has_w ? 2 * bytes : bytes);
-        bulk_g2s(s_col, a.g.col + lo16, bytes, bar);
-        if (has_w) bulk_g2s(s_w, a.g.w + lo16, bytes, bar);
-    }
-    const i64 plain_from = bytes ? max(hi16, j0) : j0;
-    for (i64 j = plain_from + threadIdx.x; j < j1; j += SPLIT_THREADS) {
-        s_col[j - lo16] = a.g.col[j];
-        if (has_w) s_w[j - lo16] = a.g.w[j];
-    }
-    // one thread waits (bounded) for the bulk copy and tells the block
-    __shared__ int staged;
-    if (threadIdx.x == 0) {
-        bool done = bytes == 0;
-        for (u32 it = 0; it < SPLIT_WAIT_LIMIT && !done; it++) done = mbar_try_wait(bar, 0);
-        if (!done) {
-            // never expected: report, wait (bounded) for the copy that still
-            // targets this block's shared memory, and give up the chunk
-            atomicExch(a.err, (int)DEV_ERR_WAIT);
-            for (u32 it = 0; it < SPLIT_WAIT_LIMIT && !done; it++) done = mbar_try_wait(bar, 0);
-        }
-        staged = done ? 1 : 0;
-    }
-    __syncthreads();
-    if (!staged) return;
+    const i64 lo16 = j0 & ~(i64)3;
+    if (!stage_rows(a.g.col, has_w ? a.g.w : (const W*)nullptr, j0, j1, s_col, s_w, bar, a.err)) return;
     const int l = lane_id(), w = threadIdx.x >> 5;
     const i64 len = j1 - j0, base = j0 - lo16;
     for (i64 t = (i64)w * 32 + l; t - l < len; t += SPLIT_THREADS) {

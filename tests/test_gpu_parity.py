@@ -384,3 +384,29 @@ def test_select_pass_hub_row_at_unaligned_offset(mem, weighted, fr):
     assert ko == kg
     assert np.array_equal(do, dg)
     assert np.array_equal(go.view(np.int32), gg_.view(np.int32))
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_build_coarse_graph_wide_row_at_unaligned_offset(mem, weighted):
+    """The 40,000-neighbour coarse row is the fourth coarse vertex, so its flat
+    member-edge list starts 3 entries in (not on a 16-byte boundary): the split
+    contraction stages its chunks by bulk copies of the aligned middle and
+    plain loads of the rest."""
+    leaves = 40000
+    rng = np.random.default_rng(5)
+    w = rng.uniform(0.5, 1.5, leaves).astype(np.float32) if weighted else None
+    hg = G.from_edges(leaves + 1, [(0, i) for i in range(1, leaves + 1)], w)
+    obj = pg.OBJ_WMOD if weighted else pg.OBJ_MOD
+    og, wg = _pair(mem, hg, obj)
+    vcmap = np.empty(leaves + 1, np.int32)
+    vcmap[0] = 3
+    vcmap[1:4] = [0, 1, 2]
+    vcmap[4] = 3
+    vcmap[5:] = np.arange(4, leaves, dtype=np.int32)
+    nc = leaves
+    co = O.build_coarse_graph(og, vcmap, nc)
+    cg = pg.build_coarse_graph(mem, wg, vcmap, nc)
+    for x, y in zip(co.arrays(), cg.to_host()):
+        assert np.array_equal(x, y)
+    rg = cg.to_host()[0]
+    assert rg[4] - rg[3] == leaves - 1
