@@ -476,10 +476,13 @@ __global__ void __launch_bounds__(256) k_place_warp(const i32* list, const i64* 
     }
 }
 
-// 32 < u <= PW_MAX: the warp stages the row in shared memory and each lane
-// ranks its entries against all of them
+// 32 < u <= PW_MAX: the warp stages the row in shared memory; up to 64
+// entries each lane ranks its entries against all of them, above that the
+// warp sorts (key, value) pairs with a bitonic network over next_pow2(u)
+// slots padded with INT_MAX keys (the keys of a row are distinct columns)
 constexpr int PW_MAX = 256;
 constexpr int PW_WARPS = 8;
+constexpr int PW_RANK_MAX = 64;
 
 template <class W>
 __global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* list, const i64* d_count, const i64* P,
@@ -487,7 +490,9 @@ __global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* li
                                                                    const i64* rowptr, const i32* skey,
                                                                    const typename Traits<W>::V* sval, i32* col,
                                                                    W* wout) {
+    using V = typename Traits<W>::V;
     __shared__ i32 kk[PW_WARPS][PW_MAX];
+    __shared__ V vv[PW_WARPS][PW_MAX];
     const int l = lane_id(), w = threadIdx.x >> 5;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
@@ -496,14 +501,48 @@ __global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* li
         i32 c = list[x];
         i64 src = P[cstart[c]];
         int u = (int)ucount[c];
-        for (int s = l; s < u; s += 32) kk[w][s] = skey[src + s];
+        if (u <= PW_RANK_MAX) {
+            for (int s = l; s < u; s += 32) kk[w][s] = skey[src + s];
+            __syncwarp();
+            for (int s = l; s < u; s += 32) {
+                i32 key = kk[w][s];
+                int rank = 0;
+                for (int t = 0; t < u; t++) rank += kk[w][t] < key ? 1 : 0;
+                col[rowptr[c] + rank] = key;
+                wout[rowptr[c] + rank] = to_w<W>(sval[src + s]);
+            }
+            __syncwarp();
+            continue;
+        }
+        const int T = (int)next_pow2_u32((u32)u);
+        for (int s = l; s < T; s += 32) {
+            kk[w][s] = s < u ? skey[src + s] : 2147483647;
+            vv[w][s] = s < u ? sval[src + s] : V(0);
+        }
         __syncwarp();
+        for (int k = 2; k <= T; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int t = l; t < T; t += 32) {
+                    const int q = t ^ j;
+                    if (q > t) {
+                        const bool up = (t & k) == 0;
+                        const i32 a0 = kk[w][t], a1 = kk[w][q];
+                        if ((a0 > a1) == up) {
+                            kk[w][t] = a1;
+                            kk[w][q] = a0;
+                            const V v0 = vv[w][t];
+                            vv[w][t] = vv[w][q];
+                            vv[w][q] = v0;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        const i64 dst = rowptr[c];
         for (int s = l; s < u; s += 32) {
-            i32 key = kk[w][s];
-            int rank = 0;
-            for (int t = 0; t < u; t++) rank += kk[w][t] < key ? 1 : 0;
-            col[rowptr[c] + rank] = key;
-            wout[rowptr[c] + rank] = to_w<W>(sval[src + s]);
+            col[dst + s] = kk[w][s];
+            wout[dst + s] = to_w<W>(vv[w][s]);
         }
         __syncwarp();
     }

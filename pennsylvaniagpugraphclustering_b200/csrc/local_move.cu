@@ -1521,11 +1521,22 @@ __global__ void k_objective(LMScalars<V>* sc, double lambda) {
     }
 }
 
-template <class T, class V>
-__global__ void k_copy_if_improved(T* dst, const T* src, i64 n, const LMScalars<V>* sc, int use_label_count) {
+// best state <- current state when the sweep improved the objective: the
+// partition, the cluster volumes (label_count of them) and the own-cluster
+// weights, in one grid-stride pass
+template <class V>
+__global__ void k_copy_if_improved(i32* best_part, const i32* part, V* td_best, const V* td, V* pv_best, const V* pv,
+                                   i64 n, const LMScalars<V>* sc) {
     if (!sc->improved) return;
-    i64 k = use_label_count ? sc->label_count : n;
-    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < k; i += (i64)gridDim.x * blockDim.x) dst[i] = src[i];
+    const i64 L = sc->label_count;
+    const i64 k = n > L ? n : L;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < k; i += (i64)gridDim.x * blockDim.x) {
+        if (i < n) {
+            best_part[i] = part[i];
+            pv_best[i] = pv[i];
+        }
+        if (i < L) td_best[i] = td[i];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2176,12 +2187,8 @@ struct Mover {
 
     void copy_if_improved(i32* best_part, V* td_best, i64 label_bound) {
         LMScalars<V>* s = sc.p;
-        k_copy_if_improved<i32, V><<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(best_part, part.p, n, s, 0);
-        PGGC_LAUNCH_CHECK();
-        k_copy_if_improved<V, V><<<grid_for(ctx, label_bound, 256), 256, 0, ctx.stream>>>(td_best, td_curr.p,
-                                                                                           label_bound, s, 1);
-        PGGC_LAUNCH_CHECK();
-        k_copy_if_improved<V, V><<<grid_for(ctx, n, 256), 256, 0, ctx.stream>>>(pvals_clone.p, pvals.p, n, s, 0);
+        k_copy_if_improved<V><<<grid_for(ctx, std::max<i64>(n, label_bound), 256), 256, 0, ctx.stream>>>(
+            best_part, part.p, td_best, td_curr.p, pvals_clone.p, pvals.p, n, s);
         PGGC_LAUNCH_CHECK();
     }
 

@@ -126,6 +126,34 @@ struct ArrOutExcl {
     __device__ void operator()(i64 i, i64 excl, i64) const { a[i] = excl; }
 };
 
+// the whole scan in one block when it fits one tile: the tile apply with a
+// zero tile offset that also writes the grand total (one launch instead of
+// three and a memset, for the many short scans of small levels)
+template <class In, class Epi>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_single(In in, Epi epi, const i64* d_k, i64 k_max,
+                                                               i64* d_total) {
+    __shared__ i64 red[SCAN_THREADS / 32 + 1];
+    i64 k = d_k ? min(*d_k, k_max) : k_max;
+    i64 base = (i64)threadIdx.x * SCAN_ITEMS;
+    i64 v[SCAN_ITEMS];
+    i64 s = 0;
+#pragma unroll
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        i64 i = base + it;
+        v[it] = (i < k) ? in(i) : 0;
+        s += v[it];
+    }
+    i64 tot;
+    i64 off = block_excl_scan_i64<SCAN_THREADS>(s, red, &tot);
+#pragma unroll
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        i64 i = base + it;
+        if (i < k) epi(i, off, v[it]);
+        off += v[it];
+    }
+    if (d_total && threadIdx.x == 0) *d_total = tot;
+}
+
 static __global__ void k_scan_total(const i64* tile_off, const i64* partial, i64 nt, i64* d_total) {
     *d_total = tile_off[nt - 1] + partial[nt - 1];
 }
@@ -140,14 +168,15 @@ void scan_apply(Context& ctx, In in, Epi epi, i64 k_max, const i64* d_k, i64* d_
         return;
     }
     i64 nt = ceil_div(k_max, SCAN_TILE);
+    if (nt == 1) {
+        k_scan_single<In, Epi><<<1, SCAN_THREADS, 0, ctx.stream>>>(in, epi, d_k, k_max, d_total);
+        PGGC_LAUNCH_CHECK();
+        return;
+    }
     Tmp<i64> partial(ctx, nt), tile_off(ctx, nt);
     k_scan_tile_sums<In><<<(unsigned)nt, SCAN_THREADS, 0, ctx.stream>>>(in, d_k, k_max, partial.p);
     PGGC_LAUNCH_CHECK();
-    if (nt == 1) {
-        PGGC_CUDA(cudaMemsetAsync(tile_off.p, 0, sizeof(i64), ctx.stream));
-    } else {
-        scan_apply(ctx, ArrIn{partial.p}, ArrOutExcl{tile_off.p}, nt, nullptr, nullptr);
-    }
+    scan_apply(ctx, ArrIn{partial.p}, ArrOutExcl{tile_off.p}, nt, nullptr, nullptr);
     k_scan_tile_apply<In, Epi><<<(unsigned)nt, SCAN_THREADS, 0, ctx.stream>>>(in, epi, d_k, k_max, tile_off.p);
     PGGC_LAUNCH_CHECK();
     if (d_total) {
