@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--cpu-sample-n", type=int, default=262144)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None, help="e2e batch size (default: --streams)")
+    ap.add_argument("--eval-ex-iters", type=int, default=8,
+                    help="filter-eval workload: improvement passes after the first (-1: until stable)")
     ap.add_argument("--by-level", action="store_true",
                     help="profiled run also splits each kernel family by multilevel level (adds 'by_level')")
     ap.add_argument("--ex-iters", type=int, default=-1,
@@ -715,10 +717,12 @@ def population(args):
 
 
 def filter_eval(args):
-    """The learned filter on unseen graphs (seed 99): R-MAT scale 25 (Mod) and a
-    DC-SBM with n = 16,777,216 at mu = 0.5 (WMod, FP32 weights), pLeiden+ until
-    stable, one run plain and one with the filter (and its judge), one stream,
-    CUDA events.  The filter is trained as for the headline line."""
+    """The learned filter on unseen graphs (seed 99): a DC-SBM with
+    n = 16,777,216 at mu = 0.5 (WMod, FP32 weights) and R-MAT scale 25 (Mod),
+    pLeiden+ with --eval-ex-iters improvement passes (until stable takes
+    minutes per run at these sizes), one run plain and one with the filter
+    (and its judge), one stream, CUDA events.  The filter is trained as for the
+    headline line."""
     import torch
     import pennsylvaniagpugraphclustering_b200 as pg
     from pennsylvaniagpugraphclustering_b200 import graphgen as gg, move_filter as MF
@@ -729,7 +733,8 @@ def filter_eval(args):
     MF.scope(mem, -1, args.filter_min_level)
     out = {"metric": "Leiden edges/s, learned filter vs plain on unseen seed-99 graphs", "unit": UNIT,
            "filter": dict(info, min_level=args.filter_min_level), "graphs": {}}
-    for name in ("rmat25", "dcsbm16m"):
+    out["ex_iters"] = args.eval_ex_iters
+    for name in ("dcsbm16m", "rmat25"):
         t0 = time.perf_counter()
         if name == "rmat25":
             h = gg.rmat(25, 16, 0.57, 0.19, 0.19, 99)
@@ -750,7 +755,8 @@ def filter_eval(args):
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                lab, st = pg.run_clustering(mem, g, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=-1, seed=99)
+                lab, st = pg.run_clustering(mem, g, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=args.eval_ex_iters,
+                                            seed=99)
                 e1.record(stream)
                 e1.synchronize()
                 ms = e0.elapsed_time(e1)

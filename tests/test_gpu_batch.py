@@ -101,9 +101,12 @@ def test_autotuner_picks_the_fastest_trial_and_keeps_results(mem):
     try:
         best, trials = pg.batch_autotune(mem, jobs)
         assert len(trials) >= 9
-        fastest = min(trials, key=lambda t: t["seconds"])
-        for k in ("thread_max_deg", "warp_max_deg", "load_factor", "streams"):
-            assert best[k] == fastest[k]
+        # a challenger replaces the incumbent only when more than 2 % faster,
+        # so the kept configuration is within 2 % of the fastest trial
+        keys = ("thread_max_deg", "warp_max_deg", "load_factor", "streams")
+        fastest = min(t["seconds"] for t in trials)
+        mine = [t["seconds"] for t in trials if all(t[k] == best[k] for k in keys)]
+        assert mine and min(mine) * 0.98 <= fastest * (1 + 1e-9)
         assert pg.tune_get(mem) == best
         # streams = 0: the tuned width; results equal sequential runs
         res = pg.batch_run(mem, jobs, streams=0)
