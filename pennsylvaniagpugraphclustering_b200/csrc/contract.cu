@@ -17,8 +17,11 @@
 //     with a global table for the rows that overflow it; weights are summed
 //     exactly (int64 / FP64);
 //  5. a prefix sum of the unique counts gives the coarse row offsets;
-//  6. each row is sorted by column (warp rank sort, block bitonic sort in shared
-//     memory, LSD radix sort for rows above 4096 entries) and written out.
+//  6. each row is sorted by column and written out: register ranks (<= 32
+//     entries), chunk ranks (sorted 32-key chunks plus binary searches into the
+//     other chunks; warp <= 256, block <= 1024 entries), bitmap ranks when the
+//     coarse graph has at most 262,144 vertices, block bitonic sort (<= 4096)
+//     and LSD radix sort above.
 // The output is the canonical (row, col)-sorted coarse CSR.
 #include <optional>
 #include "kernels.cuh"
@@ -476,13 +479,40 @@ __global__ void __launch_bounds__(256) k_place_warp(const i32* list, const i64* 
     }
 }
 
-// 32 < u <= PW_MAX: the warp stages the row in shared memory; up to 64
-// entries each lane ranks its entries against all of them, above that the
-// warp sorts (key, value) pairs with a bitonic network over next_pow2(u)
-// slots padded with INT_MAX keys (the keys of a row are distinct columns)
+// Sorting by chunk ranks: the row's entries go in chunks of 32 (one warp
+// each); a chunk is sorted by ranking every key against the chunk's other keys
+// with shuffles (ties between padding keys broken by lane, so every slot of a
+// chunk is written) and stored in shared memory; an entry's place in the row
+// is its rank in its own chunk plus, for every other chunk, the number of that
+// chunk's keys below it (a 6-step binary search of 32 sorted keys).  The keys
+// of a row are distinct columns.  Cost per entry: 32 shuffles + 6 reads per
+// other chunk, against the log^2 stages of a bitonic network.
+constexpr i32 KEY_PAD = 2147483647;  // pads chunks; coarse ids are below it
+
+__device__ __forceinline__ int chunk_rank(i32 key) {
+    const int l = lane_id();
+    int r = 0;
+#pragma unroll
+    for (int t = 0; t < 32; t++) {
+        const i32 o = __shfl_sync(FULL, key, t);
+        r += (o < key || (o == key && t < l)) ? 1 : 0;
+    }
+    return r;
+}
+
+// number of keys below `key` in a sorted chunk of 32 (padded with KEY_PAD)
+__device__ __forceinline__ int chunk_below(const i32* ck, i32 key) {
+    int pos = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1)
+        if (ck[pos + step - 1] < key) pos += step;
+    return pos + (ck[pos] < key ? 1 : 0);
+}
+
+// 32 < u <= PW_MAX: a warp per row, entries held in registers (lane l has
+// entries l, l + 32, ...), chunks sorted into shared memory, ranks summed
 constexpr int PW_MAX = 256;
 constexpr int PW_WARPS = 8;
-constexpr int PW_RANK_MAX = 64;
 
 template <class W>
 __global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* list, const i64* d_count, const i64* P,
@@ -491,60 +521,116 @@ __global__ void __launch_bounds__(PW_WARPS * 32) k_place_warp_rank(const i32* li
                                                                    const typename Traits<W>::V* sval, i32* col,
                                                                    W* wout) {
     using V = typename Traits<W>::V;
+    constexpr int NCH = PW_MAX / 32;
     __shared__ i32 kk[PW_WARPS][PW_MAX];
-    __shared__ V vv[PW_WARPS][PW_MAX];
     const int l = lane_id(), w = threadIdx.x >> 5;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
     const i64 count = *d_count;
     for (i64 x = gw; x < count; x += nw) {
-        i32 c = list[x];
-        i64 src = P[cstart[c]];
-        int u = (int)ucount[c];
-        if (u <= PW_RANK_MAX) {
-            for (int s = l; s < u; s += 32) kk[w][s] = skey[src + s];
-            __syncwarp();
-            for (int s = l; s < u; s += 32) {
-                i32 key = kk[w][s];
-                int rank = 0;
-                for (int t = 0; t < u; t++) rank += kk[w][t] < key ? 1 : 0;
-                col[rowptr[c] + rank] = key;
-                wout[rowptr[c] + rank] = to_w<W>(sval[src + s]);
-            }
-            __syncwarp();
-            continue;
-        }
-        const int T = (int)next_pow2_u32((u32)u);
-        for (int s = l; s < T; s += 32) {
-            kk[w][s] = s < u ? skey[src + s] : 2147483647;
-            vv[w][s] = s < u ? sval[src + s] : V(0);
-        }
-        __syncwarp();
-        for (int k = 2; k <= T; k <<= 1) {
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int t = l; t < T; t += 32) {
-                    const int q = t ^ j;
-                    if (q > t) {
-                        const bool up = (t & k) == 0;
-                        const i32 a0 = kk[w][t], a1 = kk[w][q];
-                        if ((a0 > a1) == up) {
-                            kk[w][t] = a1;
-                            kk[w][q] = a0;
-                            const V v0 = vv[w][t];
-                            vv[w][t] = vv[w][q];
-                            vv[w][q] = v0;
-                        }
-                    }
-                }
-                __syncwarp();
-            }
-        }
+        const i32 c = list[x];
+        const i64 src = P[cstart[c]];
+        const int u = (int)ucount[c];
         const i64 dst = rowptr[c];
-        for (int s = l; s < u; s += 32) {
-            col[dst + s] = kk[w][s];
-            wout[dst + s] = to_w<W>(vv[w][s]);
+        const int nch = (u + 31) >> 5;
+        i32 key[NCH];
+        V val[NCH];
+        int rk[NCH];
+#pragma unroll
+        for (int k = 0; k < NCH; k++) {
+            const int s = 32 * k + l;
+            key[k] = s < u ? skey[src + s] : KEY_PAD;
+            val[k] = s < u ? sval[src + s] : V(0);
+        }
+#pragma unroll
+        for (int k = 0; k < NCH; k++) {
+            if (k < nch) {
+                rk[k] = chunk_rank(key[k]);
+                kk[w][32 * k + rk[k]] = key[k];
+            }
         }
         __syncwarp();
+        // chunk by chunk, the searches of all the lane's entries together (independent, so
+        // their shared-memory reads overlap)
+        int g[NCH];
+#pragma unroll
+        for (int k = 0; k < NCH; k++) g[k] = k < nch ? rk[k] : 0;
+        for (int j = 0; j < nch; j++) {
+            const i32* ck = &kk[w][32 * j];
+#pragma unroll
+            for (int k = 0; k < NCH; k++)
+                if (k < nch && k != j) g[k] += chunk_below(ck, key[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < NCH; k++) {
+            if (k < nch && 32 * k + l < u) {
+                col[dst + g[k]] = key[k];
+                wout[dst + g[k]] = to_w<W>(val[k]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// PW_MAX < u <= PB_MID: the same with a 256-thread block per row (warp w
+// sorts chunks w, w + 8, ...)
+constexpr int PBR_THREADS = 256;
+
+template <class W>
+__global__ void __launch_bounds__(PBR_THREADS) k_place_block_rank(const i32* list, const i64* d_count, const i64* P,
+                                                                  const i64* cstart, const i64* ucount,
+                                                                  const i64* rowptr, const i32* skey,
+                                                                  const typename Traits<W>::V* sval, i32* col,
+                                                                  W* wout) {
+    using V = typename Traits<W>::V;
+    constexpr int CAP = 1024, PER = CAP / PBR_THREADS;
+    __shared__ i32 kk[CAP];
+    const int t = threadIdx.x;
+    const i64 count = *d_count;
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        const i32 c = list[x];
+        const i64 src = P[cstart[c]];
+        const int u = (int)ucount[c];
+        const i64 dst = rowptr[c];
+        const int nch = (u + 31) >> 5;
+        i32 key[PER];
+        V val[PER];
+        int rk[PER];
+#pragma unroll
+        for (int m = 0; m < PER; m++) {
+            const int s = t + PBR_THREADS * m;
+            key[m] = s < u ? skey[src + s] : KEY_PAD;
+            val[m] = s < u ? sval[src + s] : V(0);
+        }
+#pragma unroll
+        for (int m = 0; m < PER; m++) {
+            const int k = (t + PBR_THREADS * m) >> 5;  // warp-uniform
+            if (k < nch) {
+                rk[m] = chunk_rank(key[m]);
+                kk[32 * k + rk[m]] = key[m];
+            }
+        }
+        __syncthreads();
+        int g[PER];
+#pragma unroll
+        for (int m = 0; m < PER; m++) g[m] = ((t + PBR_THREADS * m) >> 5) < nch ? rk[m] : 0;
+        for (int j = 0; j < nch; j++) {
+            const i32* ck = &kk[32 * j];
+#pragma unroll
+            for (int m = 0; m < PER; m++) {
+                const int k = (t + PBR_THREADS * m) >> 5;
+                if (k < nch && k != j) g[m] += chunk_below(ck, key[m]);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < PER; m++) {
+            const int s = t + PBR_THREADS * m;
+            if (s < u) {
+                col[dst + g[m]] = key[m];
+                wout[dst + g[m]] = to_w<W>(val[m]);
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -982,22 +1068,24 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     }
     const bool bitmap = nc <= BM_MAX_NC;
     if (bitmap) {
-        // every row above 32 entries: bitmap ranks (lists pr, pb, pb2, ph)
+        // every row above PW_MAX entries: bitmap ranks (lists pb, pb2, ph)
         const int nwords = (int)ceil_div(nc, 32);
         const size_t smem = sizeof(u32) * 2 * (size_t)nwords;
         set_dynamic_smem_once(k_place_bitmap<W>, (int)(sizeof(u32) * 2 * ceil_div(BM_MAX_NC, 32)), ctx.device);
-        const i64 lists[4] = {p_r, p_b, p_b2, p_h};
-        i32* lp[4] = {pr.p, pb.p, pb2.p, ph.p};
-        for (int q = 0; q < 4; q++) {
+        const i64 lists[3] = {p_b, p_b2, p_h};
+        i32* lp[3] = {pb.p, pb2.p, ph.p};
+        for (int q = 0; q < 3; q++) {
             if (lists[q] <= 0) continue;
             int grid = (int)std::min<i64>(lists[q], (i64)ctx.num_sms * 4);
-            k_place_bitmap<W><<<grid, BM_THREADS, smem, ctx.stream>>>(lp[q], counts.p + 8 + q, P.p, cstart.p, ucount.p,
+            k_place_bitmap<W><<<grid, BM_THREADS, smem, ctx.stream>>>(lp[q], counts.p + 9 + q, P.p, cstart.p, ucount.p,
                                                                      cg->rowptr.p, okey.p, oval.p, cg->col.p,
                                                                      cg->w.p, nwords);
             PGGC_LAUNCH_CHECK();
         }
     }
-    if (!bitmap && p_r > 0) {
+    // rows of 33..PW_MAX entries: chunk ranks in a warp (cheaper than the
+    // bitmap's O(nc / 32) per row even for small nc)
+    if (p_r > 0) {
         int grid = (int)std::min<i64>(ceil_div(p_r, PW_WARPS), (i64)ctx.num_sms * 8);
         k_place_warp_rank<W><<<grid, PW_WARPS * 32, 0, ctx.stream>>>(pr.p, counts.p + 8, P.p, cstart.p, ucount.p,
                                                                      cg->rowptr.p, okey.p, oval.p, cg->col.p,
@@ -1006,8 +1094,9 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     }
     if (!bitmap && p_b > 0) {
         int grid = (int)std::min<i64>(p_b, (i64)ctx.num_sms * 8);
-        k_place_block<W, 256, PB_MID><<<grid, 256, 0, ctx.stream>>>(pb.p, counts.p + 9, P.p, cstart.p, ucount.p,
-                                                                    cg->rowptr.p, okey.p, oval.p, cg->col.p, cg->w.p);
+        k_place_block_rank<W><<<grid, PBR_THREADS, 0, ctx.stream>>>(pb.p, counts.p + 9, P.p, cstart.p, ucount.p,
+                                                                     cg->rowptr.p, okey.p, oval.p, cg->col.p,
+                                                                     cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
     if (!bitmap && p_b2 > 0) {

@@ -174,23 +174,74 @@ __global__ void __launch_bounds__(256) k_pick_heavy_warp(PickArgs<W> a, const i3
     }
 }
 
+// One thread per vertex of low degree (the degree classes up to 32): per
+// chunk of 8 edges the columns, constraints and well flags are gathered
+// together, then the edges are evaluated in order; the argmax order (sample,
+// then edge index) is total, so this equals the warp kernel's pick.
+template <class W>
+__global__ void __launch_bounds__(256, 3) k_pick_heavy_thr(PickArgs<W> a, Range rg) {
+    const i64 lo = rg.begin(), hi = rg.end();
+    for (i64 x = lo + blockIdx.x * (i64)blockDim.x + threadIdx.x; x < hi; x += (i64)gridDim.x * blockDim.x) {
+        const i32 i = rg.list[x];
+        const u32 h = murmur3_32(a.seed + (u32)i);
+        if (h % 10000u == 0 || !a.well[i]) {
+            a.hn[i] = i;
+            continue;
+        }
+        const i64 b = a.g.rowptr[i], e = a.g.rowptr[i + 1];
+        const float multi = a.gamma * to_f(a.g.vtx_w[i]);
+        const i32 ci = a.constraint[i];
+        float bs = -1.0f;
+        i64 bj = -1;
+        // edges in chunks of 8, in order
+#pragma unroll 1
+        for (i64 c0 = b; c0 < e; c0 += 8) {
+            i32 cv[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) cv[t] = c0 + t < e ? a.g.col[c0 + t] : -1;
+            bool ok[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) ok[t] = cv[t] >= 0 && a.constraint[cv[t]] == ci;
+#pragma unroll
+            for (int t = 0; t < 8; t++) ok[t] = ok[t] && a.well[cv[t]];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                if (!ok[t]) continue;
+                const i64 j = c0 + t;
+                const float val = (float)a.g.wgt(j) - multi * to_f(a.g.vtx_w[cv[t]]);
+                if (val >= 0.0f) {
+                    float sample = fabsf((float)murmur3_32(a.seed + (u32)(u64)j) / (float)ORD_MAX);
+                    const float v2 = val * val;
+                    sample = sample * (v2 * v2);
+                    if (sample >= 0.0f && sample_better(sample, j, bs, bj)) {
+                        bs = sample;
+                        bj = j;
+                    }
+                }
+            }
+        }
+        a.hn[i] = bj >= b ? a.g.col[bj] : i;
+    }
+}
+
 // G-lane groups for low-degree vertices (NG = 32 / G vertices per warp); the
 // argmax order (sample, then edge index) is total, so any split of the edges
 // over lanes gives the warp kernel's pick
 template <class W, int G>
-__global__ void __launch_bounds__(256) k_pick_heavy_grp(PickArgs<W> a, const i32* list, i64 count) {
+__global__ void __launch_bounds__(256) k_pick_heavy_grp(PickArgs<W> a, Range rg) {
     constexpr int NG = 32 / G;
     const int l = lane_id(), r = l & (G - 1), grp = l / G;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
-    for (i64 base = gw * NG; base < count; base += nw * NG) {
+    const i64 lo = rg.begin(), count = rg.end();
+    for (i64 base = lo + gw * NG; base < count; base += nw * NG) {
         const i64 x = base + grp;
         i32 i = -1;
         bool act = false;
         i64 b = 0, e = 0;
         float multi = 0.f;
         if (x < count) {
-            i = list[x];
+            i = rg.list[x];
             const u32 h = murmur3_32(a.seed + (u32)i);
             if (h % 10000u == 0 || !a.well[i]) {
                 if (r == 0) a.hn[i] = i;
@@ -360,14 +411,48 @@ __device__ __forceinline__ typename Traits<W>::V inner_term(const DGraph<W>& g, 
     return (vcmap[i] == vcmap[v] && order[v] < order[i]) ? V(g.wgt(j)) : V(0);
 }
 
+// Vertices of degree <= 2H (H = 8: degree classes 0 and 1, H = 16: class 2),
+// one thread each: the 32-lane canonical association of the row's terms
+// (canon_tree), no shuffles; the order of the neighbour is read only when
+// its tree matches.
+template <class W, int H>
+__global__ void __launch_bounds__(256) k_inner_thr(DGraph<W> g, Range rg, const i32* vcmap, const i32* order,
+                                                   typename Traits<W>::V* inner) {
+    using V = typename Traits<W>::V;
+    const i64 lo = rg.begin(), hi = rg.end();
+    for (i64 x = lo + blockIdx.x * (i64)blockDim.x + threadIdx.x; x < hi; x += (i64)gridDim.x * blockDim.x) {
+        const i32 i = rg.list[x];
+        const i64 b = g.rowptr[i], e = g.rowptr[i + 1];
+        const i32 ci = vcmap[i], oi = order[i];
+        i32 cv[2 * H];
+#pragma unroll
+        for (int t = 0; t < 2 * H; t++) cv[t] = b + t < e ? g.col[b + t] : -1;
+        bool in[2 * H];
+#pragma unroll
+        for (int t = 0; t < 2 * H; t++) in[t] = cv[t] >= 0 && vcmap[cv[t]] == ci;
+#pragma unroll
+        for (int t = 0; t < 2 * H; t++) in[t] = in[t] && order[cv[t]] < oi;
+        V acc[H];
+#pragma unroll
+        for (int r = 0; r < H; r++) {
+            acc[r] = V(0);
+            if (b + r < e) acc[r] += in[r] ? V(g.wgt(b + r)) : V(0);
+            if (b + r + H < e) acc[r] += in[r + H] ? V(g.wgt(b + r + H)) : V(0);
+        }
+        inner[i] = canon_tree<H, V>(acc);
+    }
+}
+
+// warp per vertex (degree below MASSIVE_CUTOFF): the canonical warp sum
 template <class W>
-__global__ void __launch_bounds__(256) k_inner_warp(DGraph<W> g, const i32* list, i64 count, const i32* vcmap,
-                                                    const i32* order, typename Traits<W>::V* inner) {
+__global__ void __launch_bounds__(256) k_inner_warp(DGraph<W> g, Range rg, const i32* vcmap, const i32* order,
+                                                    typename Traits<W>::V* inner) {
     using V = typename Traits<W>::V;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
-    for (i64 x = gw; x < count; x += nw) {
-        i32 i = list[x];
+    const i64 lo = rg.begin(), hi = rg.end();
+    for (i64 x = lo + gw; x < hi; x += nw) {
+        i32 i = rg.list[x];
         V r = VSum<V>::warp(g.rowptr[i], g.rowptr[i + 1], [&](i64 j) { return inner_term(g, vcmap, order, i, j); });
         if (lane_id() == 0) inner[i] = r;
     }
@@ -548,10 +633,16 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
             PGGC_LAUNCH_CHECK();
         }
     } else {
-        // degree < 128: 8-lane groups; 128 <= degree < 15000: a warp per vertex
+        // degree <= 32 (classes 0-2 of the graph's class lists): a thread per
+        // vertex; 32 < degree < 128 (class 3): 8-lane groups; 128 <= degree <
+        // 15000: a warp per vertex
         if (ord.off_large > 0) {
+            const ClassLists cls = graph_class_lists<W>(ctx, g, ord);
+            const int gt = (int)std::min<i64>(ceil_div(ord.off_large, 256), (i64)ctx.num_sms * 16);
+            k_pick_heavy_thr<W><<<gt, 256, 0, ctx.stream>>>(pa, dev_range(cls.list, cls.off + 0, cls.off + 3));
+            PGGC_LAUNCH_CHECK();
             const int g8 = (int)std::min<i64>(ceil_div(ord.off_large, 32), (i64)ctx.num_sms * 16);
-            k_pick_heavy_grp<W, 8><<<g8, 256, 0, ctx.stream>>>(pa, small_list, ord.off_large);
+            k_pick_heavy_grp<W, 8><<<g8, 256, 0, ctx.stream>>>(pa, dev_range(cls.list, cls.off + 3, cls.off + 4));
             PGGC_LAUNCH_CHECK();
         }
         if (nsmall > ord.off_large) {
@@ -596,8 +687,24 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
         PGGC_LAUNCH_CHECK();
     }
     if (nsmall > 0) {
-        k_inner_warp<W><<<gw, 256, 0, ctx.stream>>>(gv, small_list, nsmall, vcmap.p, order.p, inner.p);
+        // degree <= 32 (classes 0-2 of the graph's class lists): a thread per
+        // vertex; 32 < degree < 128 (class 3) and up to MASSIVE_CUTOFF: a warp
+        const ClassLists cls = graph_class_lists<W>(ctx, g, ord);
+        const int gt = (int)std::min<i64>(ceil_div(std::max<i64>(nsmall, 1), 256), (i64)ctx.num_sms * 16);
+        k_inner_thr<W, 8><<<gt, 256, 0, ctx.stream>>>(gv, dev_range(cls.list, cls.off + 0, cls.off + 2), vcmap.p,
+                                                      order.p, inner.p);
         PGGC_LAUNCH_CHECK();
+        k_inner_thr<W, 16><<<gt, 256, 0, ctx.stream>>>(gv, dev_range(cls.list, cls.off + 2, cls.off + 3), vcmap.p,
+                                                       order.p, inner.p);
+        PGGC_LAUNCH_CHECK();
+        k_inner_warp<W><<<gw, 256, 0, ctx.stream>>>(gv, dev_range(cls.list, cls.off + 3, cls.off + 4), vcmap.p,
+                                                    order.p, inner.p);
+        PGGC_LAUNCH_CHECK();
+        if (nsmall > ord.off_large) {
+            k_inner_warp<W><<<gw, 256, 0, ctx.stream>>>(gv, host_range(small_list, ord.off_large, nsmall), vcmap.p,
+                                                        order.p, inner.p);
+            PGGC_LAUNCH_CHECK();
+        }
     }
     if (nmass > 0) {
         k_inner_block<W><<<gb, 1024, 0, ctx.stream>>>(gv, mass_list, nmass, vcmap.p, order.p, inner.p);

@@ -410,3 +410,63 @@ def test_build_coarse_graph_wide_row_at_unaligned_offset(mem, weighted):
         assert np.array_equal(x, y)
     rg = cg.to_host()[0]
     assert rg[4] - rg[3] == leaves - 1
+
+
+@pytest.mark.parametrize("extra", [1000, 270000])
+def test_build_coarse_graph_row_sizes_at_sort_boundaries(mem, extra):
+    """Stars whose centres become coarse rows of exactly u distinct columns,
+    for u around every boundary of the placement sorts (32-key chunks, the
+    warp's 256, the block's 1024), leaves mapped to shuffled coarse ids; with
+    1,000 or 270,000 further isolated vertices, so the coarse graph is below
+    or above the bitmap placement's 262,144 vertices."""
+    sizes = [31, 32, 33, 63, 64, 65, 100, 255, 256, 257, 511, 512, 513, 1000, 1023, 1024, 1025]
+    edges, v = [], 0
+    for u in sizes:
+        c = v
+        edges += [(c, c + 1 + k) for k in range(u)]
+        v += u + 1
+    n = v + extra
+    rng = np.random.default_rng(17)
+    w = rng.uniform(0.5, 1.5, len(edges)).astype(np.float32)
+    hg = G.from_edges(n, edges, w)
+    og, wg = _pair(mem, hg, pg.OBJ_WMOD)
+    vcmap = rng.permutation(n).astype(np.int32)  # every vertex its own coarse vertex, shuffled ids
+    co = O.build_coarse_graph(og, vcmap, n)
+    cg = pg.build_coarse_graph(mem, wg, vcmap, n)
+    for x, y in zip(co.arrays(), cg.to_host()):
+        assert np.array_equal(x, y)
+    rg = cg.to_host()[0]
+    deg = np.diff(rg)
+    for u in sizes:
+        assert (deg == u).any()
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_build_coarse_graph_member_layouts(mem, weighted):
+    """Coarse rows assembled from awkward member lists: members without edges
+    (isolated vertices) between real ones, a coarse vertex with no members,
+    rows of many members, and an overflowing row made of ~20,000 members."""
+    base = G.small_rmat(seed=5, scale=17)
+    iso = 3000
+    rowptr = np.concatenate([base.rowptr, np.full(iso, base.rowptr[-1], np.int64)])
+    w = G.symmetric_weights(base) if weighted else None
+    hg = G.HostGraph(rowptr, base.col, w, name="rmat17+isolated")
+    n0, n = base.n, hg.n
+    obj = pg.OBJ_WMOD if weighted else pg.OBJ_MOD
+    og, wg = _pair(mem, hg, obj)
+    rng = np.random.default_rng(13)
+    for nc in (300, 3000, 40000):
+        vcmap = rng.integers(1, nc, n).astype(np.int32)  # coarse vertex 0 has no members
+        vcmap[n0:n0 + 2000] = 2                          # 2000 isolated members ...
+        vcmap[40000:40100] = 2                           # ... around 100 real ones
+        vcmap[50000:53000] = 5                           # 3000 members
+        if nc == 40000:
+            vcmap[:20000] = 1                            # the R-MAT hubs: an overflowing row
+        co = O.build_coarse_graph(og, vcmap, nc)
+        cg = pg.build_coarse_graph(mem, wg, vcmap, nc)
+        for x, y in zip(co.arrays(), cg.to_host()):
+            assert np.array_equal(x, y)
+        rg = cg.to_host()[0]
+        assert rg[1] == rg[0] == 0
+        if nc == 40000:
+            assert rg[2] - rg[1] > 16384
