@@ -18,9 +18,12 @@ time (the reference's "Cluster time" span), at equal modularity:
   streams) with the learned move filter on, its judge included -- the
   batched+learned configuration.  Time = CUDA events on the context stream,
   which the batch's workers are ordered against.
-* ``plain``: R of the same seeds run one after another, no filter, one stream;
-  ``ratio_vs_plain`` = value / plain edges/s, with both modularities (mean over
-  those seeds) and the criterion "ratio >= 1.5 at modularity within 0.001".
+* ``plain``: the same seeds (all K by default, up to a wall-clock budget)
+  run one after another, no filter, one stream; ``ratio_vs_plain`` = value / plain edges/s, with both
+  modularities (mean over the seeds) and the criterion "ratio >= 1.5 at
+  modularity within 0.001".  The number of improvement passes until the
+  objective stops rising differs by up to +-30 % between seeds, so the two
+  arms run the same population.
 * ``e2e``: a batch of P members through the public C ABI from host buffers:
   CSR upload, graph + objective construction, clustering and label download.
 
@@ -77,8 +80,12 @@ def parse():
     ap.add_argument("--n", type=int, default=4194304, help="DC-SBM vertex count (default: the named workload)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--streams", type=int, default=6, help="worker streams of the batch (population width)")
-    ap.add_argument("--plain-runs", type=int, default=2,
-                    help="plain runs (the first seeds of the population, no filter, one stream) for the ratio")
+    ap.add_argument("--plain-runs", type=int, default=-1,
+                    help="plain runs for the ratio (the first seeds of the population, no filter, one stream; "
+                         "-1: every seed of the population, so both arms run the same seeds, stopping after "
+                         "--plain-budget seconds once two runs are done)")
+    ap.add_argument("--plain-budget", type=float, default=120.0,
+                    help="wall-clock bound of the plain arm when --plain-runs is -1")
     ap.add_argument("--no-filter", action="store_true", help="batched plain runs (no learned filter)")
     ap.add_argument("--recall", type=float, default=0.995,
                     help="recall on the training logs that sets the filter's logit threshold")
@@ -358,9 +365,13 @@ def ours(args):
     q_batch = [st["objective"] for _, st in res]
 
     # plain: the first R seeds, no filter, one after another on one stream
-    R = max(0, min(args.plain_runs, K))
+    R = K if args.plain_runs < 0 else max(0, min(args.plain_runs, K))
     plain_ms, plain_q, plain_passes = [], [], []
+    t_plain = time.perf_counter()
     for sd in seeds[:R]:
+        if args.plain_runs < 0 and len(plain_ms) >= 2 and time.perf_counter() - t_plain > args.plain_budget:
+            R = len(plain_ms)
+            break
         cd = pg.get_objective(mem, wg, pg.OBJ_WMOD, 1.0)
         ms, (_, st) = timed(lambda: pg.run_clustering(mem, wg, cd, method=pg.METHOD_LEIDEN_PLUS,
                                                         ex_iters=args.ex_iters, seed=sd))
@@ -415,8 +426,12 @@ def ours(args):
     E = max(0, E)
     e2e_ms = float("nan")
     if E > 0:
+        # the host CSR in pinned (page-locked) buffers, as a caller streaming
+        # graphs would hold it; pinning is outside the timed region
+        h_rowptr, h_col, h_w = (torch.from_numpy(a).pin_memory() for a in (g.rowptr, g.col, g.w))
+
         def e2e_once():
-            g2 = pg.weighted_graph(mem, g.rowptr, g.col, g.w, objective=pg.OBJ_WMOD)
+            g2 = pg.weighted_graph(mem, h_rowptr, h_col, h_w, objective=pg.OBJ_WMOD)
             if learned:
                 MF.enable(mem, params, thr)
             try:
@@ -609,12 +624,13 @@ def plain_workload(args):
     _lib.check(lib.pggc_profile_enable(mem.handle, 0))
     fam = _families(lib, _lib, mem)
     q, _ = pg.verify_objective(mem, wg, labels[:g.n].cpu().numpy(), pg.OBJ_MOD)
-    # e2e from host buffers
-    host = np.empty(g.n, np.int32)
+    # e2e from pinned host buffers (pinned outside the timed region)
+    host = torch.empty(g.n, dtype=torch.int32).pin_memory()
+    h_rowptr, h_col = torch.from_numpy(g.rowptr).pin_memory(), torch.from_numpy(g.col).pin_memory()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    g2 = pg.weighted_graph(mem, g.rowptr, g.col, None, objective=pg.OBJ_MOD)
+    g2 = pg.weighted_graph(mem, h_rowptr, h_col, None, objective=pg.OBJ_MOD)
     cd2 = pg.get_objective(mem, g2, pg.OBJ_MOD, 1.0)
     pg.run_clustering(mem, g2, cd2, method=pg.METHOD_LOUVAIN, ex_iters=0, seed=args.seed, out=host)
     e1.record(stream)
