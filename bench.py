@@ -103,7 +103,7 @@ def parse():
     ap.add_argument("--ex-iters", type=int, default=-1,
                     help="pLeiden+ passes after the first (-1: until the objective stops rising)")
     ap.add_argument("--workload", default="dcsbm4m",
-                    choices=["dcsbm4m", "rmat24", "sbm65k", "sbm-population", "filter-eval"],
+                    choices=["dcsbm4m", "rmat24", "sbm65k", "sbm-population", "filter-eval", "profile-case"],
                     help="dcsbm4m: the headline line (batched+learned vs plain pLeiden+); rmat24: plain pLouvain "
                          "on R-MAT scale 24 (contraction stress); sbm65k: plain pLouvain on the planted SBM; "
                          "sbm-population: 256 uneven SBMs, batched (autotuned) vs sequential pLeiden+; "
@@ -795,6 +795,31 @@ def filter_eval(args):
     print(json.dumps(out), flush=True)
 
 
+def profile_case(args):
+    """The small case for profiler captures: one pLeiden+ pass (ex_iters = 0)
+    on the DC-SBM n = 1,048,576 with the workload's parameters (21 M directed
+    edges, ~1 GB on the device, inputs above L2), the library's family
+    counters on; prints the contraction family's launches, time and
+    algorithmic bytes.  Not a bench line."""
+    import ctypes
+    import pennsylvaniagpugraphclustering_b200 as pg
+    from pennsylvaniagpugraphclustering_b200 import _lib, graphgen as gg
+    g = gg.dcsbm(1048576, 1, mean_deg=gg.DCSBM_4M_MEAN_DEG)
+    mem = pg.memory_store(0)
+    wg = pg.weighted_graph(mem, g.rowptr, g.col, g.w, objective=pg.OBJ_WMOD)
+    cd = pg.get_objective(mem, wg, pg.OBJ_WMOD, 1.0)
+    lib = _lib.lib()
+    _lib.check(lib.pggc_profile_enable(mem.handle, 1))
+    _, st = pg.run_clustering(mem, wg, cd, method=pg.METHOD_LEIDEN_PLUS, ex_iters=0, seed=1)
+    _lib.check(lib.pggc_profile_enable(mem.handle, 0))
+    n_l, t_ms, by = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+    _lib.check(lib.pggc_profile_read(mem.handle, b"contract", ctypes.byref(n_l), ctypes.byref(t_ms),
+                                     ctypes.byref(by)))
+    print(json.dumps({"case": "pLeiden+ first pass, DC-SBM n=1,048,576", "n": g.n, "nnz": g.nnz,
+                      "levels": st["levels"], "objective": st["objective"], "contractions": n_l.value,
+                      "contract_ms": t_ms.value, "contract_algorithmic_bytes": by.value}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -805,6 +830,8 @@ def main():
         population(args)
     elif args.workload == "filter-eval":
         filter_eval(args)
+    elif args.workload == "profile-case":
+        profile_case(args)
     else:
         plain_workload(args)
 
