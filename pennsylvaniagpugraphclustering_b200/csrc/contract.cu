@@ -20,8 +20,9 @@
 //  6. each row is sorted by column and written out: register ranks (<= 32
 //     entries), chunk ranks (sorted 32-key chunks plus binary searches into the
 //     other chunks; warp <= 256, block <= 1024 entries), bitmap ranks when the
-//     coarse graph has at most 262,144 vertices, block bitonic sort (<= 4096)
-//     and LSD radix sort above.
+//     coarse graph has at most 262,144 vertices (and for rows above 1024
+//     entries up to 928,768 vertices), block bitonic sort (<= 4096) and LSD
+//     radix sort above.
 // The output is the canonical (row, col)-sorted coarse CSR.
 #include <optional>
 #include "kernels.cuh"
@@ -698,8 +699,13 @@ __global__ void __launch_bounds__(THREADS) k_place_block(const i32* list, const 
 // comparison sort.
 constexpr i64 BM_MAX_NC = 262144;
 constexpr int BM_THREADS = 256;
+// Rows above PB_MID entries of coarse graphs up to BM_BIG_MAX_NC vertices: the
+// same with 1024 threads and a bitmap plus word prefix that fill the 227 KB a
+// block may have -- a few rows per SM, each O(nc / 32 / 1024) per thread,
+// against a 4096-slot bitonic network or the radix sort
+constexpr i64 BM_BIG_MAX_NC = 29024 * 32;
 
-template <class W>
+template <class W, int BM_THREADS = BM_THREADS>
 __global__ void __launch_bounds__(BM_THREADS) k_place_bitmap(const i32* list, const i64* d_count, const i64* P,
                                                             const i64* cstart, const i64* ucount, const i64* rowptr,
                                                             const i32* skey, const typename Traits<W>::V* sval,
@@ -1083,6 +1089,23 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
             PGGC_LAUNCH_CHECK();
         }
     }
+    const bool bitmap_big = !bitmap && nc <= BM_BIG_MAX_NC;
+    if (bitmap_big && (p_b2 > 0 || p_h > 0)) {
+        const int nwords = (int)ceil_div(nc, 32);
+        const size_t smem = sizeof(u32) * 2 * (size_t)nwords;
+        set_dynamic_smem_once(k_place_bitmap<W, 1024>, (int)(sizeof(u32) * 2 * ceil_div(BM_BIG_MAX_NC, 32)),
+                              ctx.device);
+        const i64 lists[2] = {p_b2, p_h};
+        i32* lp[2] = {pb2.p, ph.p};
+        for (int q = 0; q < 2; q++) {
+            if (lists[q] <= 0) continue;
+            int grid = (int)std::min<i64>(lists[q], (i64)ctx.num_sms);
+            k_place_bitmap<W, 1024><<<grid, 1024, smem, ctx.stream>>>(lp[q], counts.p + 10 + q, P.p, cstart.p,
+                                                                     ucount.p, cg->rowptr.p, okey.p, oval.p,
+                                                                     cg->col.p, cg->w.p, nwords);
+            PGGC_LAUNCH_CHECK();
+        }
+    }
     // rows of 33..PW_MAX entries: chunk ranks in a warp (cheaper than the
     // bitmap's O(nc / 32) per row even for small nc)
     if (p_r > 0) {
@@ -1099,14 +1122,14 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
                                                                      cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
-    if (!bitmap && p_b2 > 0) {
+    if (!bitmap && !bitmap_big && p_b2 > 0) {
         int grid = (int)std::min<i64>(p_b2, (i64)ctx.num_sms * 2);
         k_place_block<W, 1024, PB_MAX><<<grid, 1024, 0, ctx.stream>>>(pb2.p, counts.p + 10, P.p, cstart.p, ucount.p,
                                                                       cg->rowptr.p, okey.p, oval.p, cg->col.p,
                                                                       cg->w.p);
         PGGC_LAUNCH_CHECK();
     }
-    if (!bitmap && p_h > 0) {
+    if (!bitmap && !bitmap_big && p_h > 0) {
         WsBuf<u64> tk(ctx, CS_TK, tn), tk2(ctx, CS_TK2, tn);
         WsBuf<V> tv(ctx, CS_TV, tn), tv2(ctx, CS_TV2, tn);
         int grid = (int)std::min<i64>(p_h, (i64)ctx.num_sms * 4);
