@@ -68,7 +68,8 @@ Q_TOLERANCE = 0.001
 DOMINANT_FAMILIES = ("select_warp", "select_block", "select_huge", "afterburner_warp", "own_weights", "contract",
                      "leiden_refine", "filter")
 # sub-phases reported beside the families (not candidates for the roofline line)
-SUB_PHASES = ("contract_prep", "contract_hash", "contract_place", "contract_place_big", "host_alloc")
+SUB_PHASES = ("contract_prep", "contract_hash", "contract_place", "contract_place_big", "host_alloc", "lm_compact",
+              "lm_roundtrip", "lm_newids", "lm_moves", "lm_copy")
 
 
 def parse():

@@ -2323,19 +2323,35 @@ void local_move(Context& ctx, const Graph<W>& g, const Ordering& ord, i32* best_
                                     m.gain.p, &m.sc.p->label_count, pm);
                 m.label_bound_host = label_bound;
                 m.launch_select(a, constrained);
-                m.compact_candidates();
+                {
+                    ProfScope pc(ctx, "lm_compact");
+                    m.compact_candidates();
+                }
                 m.afterburner(pm);
                 m.filter_post();
-                const LMScalars<V>* hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
+                const LMScalars<V>* hs;
+                {
+                    // the GPU's idle time while the host reads the sweep's counts
+                    ProfScope pr(ctx, "lm_roundtrip");
+                    hs = (const LMScalars<V>*)ctx.readback(m.sc.p, sizeof(LMScalars<V>));
+                }
                 i64 ncand = hs->num_cand, nm = hs->num_moves;
                 const bool any_new = hs->new_hint != 0;
                 if (ncand == 0 || nm == 0) break;
                 // set_new_cluster_ids is a no-op without NEW_PART moves (src/local_mover.cpp:236)
-                if ((iter_count > 1 || !is_initial) && any_new)
+                if ((iter_count > 1 || !is_initial) && any_new) {
+                    ProfScope pn(ctx, "lm_newids");
                     m.set_new_cluster_ids(nm, constrained ? constraint : nullptr);
+                }
                 label_bound = std::min<i64>(label_bound + nm, m.cap);
-                m.perform_moves(nm, best.lambda, label_bound);
-                m.copy_if_improved(best_part, best.total_deg.p, label_bound);
+                {
+                    ProfScope pm_(ctx, "lm_moves");
+                    m.perform_moves(nm, best.lambda, label_bound);
+                }
+                {
+                    ProfScope pk(ctx, "lm_copy");
+                    m.copy_if_improved(best_part, best.total_deg.p, label_bound);
+                }
                 total_moves += nm;
             }
         }
