@@ -2015,7 +2015,11 @@ struct Mover {
                 SelArgs<W> a5 = a;
                 a5.dense = label_bound_host <= SEL_TS_MAX ? 1 : 0;
                 set_dynamic_smem_once(k_select_block<W, CON, false, 512>, (int)(slot * SEL_TS_MAX), ctx.device);
-                k_select_block<W, CON, false, 512><<<(int)n5, 512, slot * SEL_TS_MAX, ctx.stream>>>(
+                // a dense table needs only the label_bound values: more blocks fit an SM
+                const size_t smem5 =
+                    a5.dense ? sizeof(V) * (size_t)std::max<i64>(label_bound_host, 1) : slot * SEL_TS_MAX;
+                const int g5 = a5.dense ? (int)std::min<i64>(nb, (i64)ctx.num_sms * 4) : (int)n5;
+                k_select_block<W, CON, false, 512><<<g5, 512, smem5, ctx.stream>>>(
                     a5, dev_range(cls.list, cls.off + 5, cls.off + 6), nullptr, nullptr, SEL_TS_MAX);
                 PGGC_LAUNCH_CHECK();
             }
@@ -2031,10 +2035,12 @@ struct Mover {
             i64* ovf_cnt = ctx.ws_get<i64>(S_OVF_CNT, 1);
             PGGC_CUDA(cudaMemsetAsync(ovf_cnt, 0, sizeof(i64), ctx.stream));
             set_dynamic_smem_once(k_select_block<W, CON, false, 1024, true>, (int)(slot * TS), ctx.device);
-            int grid = (int)std::min<i64>(ord.n_huge, (i64)ctx.num_sms);
             SelArgs<W> ah = a;
             ah.dense = label_bound_host <= TS ? 1 : 0;
-            k_select_block<W, CON, false, 1024, true><<<grid, 1024, slot * TS, ctx.stream>>>(
+            // a dense table needs only the label_bound values: two blocks fit an SM
+            const size_t smemh = ah.dense ? sizeof(V) * (size_t)std::max<i64>(label_bound_host, 1) : slot * TS;
+            const int grid = (int)std::min<i64>(ord.n_huge, (i64)ctx.num_sms * (smemh <= 100 * 1024 ? 2 : 1));
+            k_select_block<W, CON, false, 1024, true><<<grid, 1024, smemh, ctx.stream>>>(
                 ah, host_range(ord.huge.p, 0, ord.n_huge), nullptr, nullptr, TS, ovf, ovf_cnt);
             PGGC_LAUNCH_CHECK();
             // the vertices that overflowed: rows split across blocks, in rounds
