@@ -14,8 +14,9 @@
 //     shared table, __match_any_sync chunk pre-aggregation), a block with a
 //     2048- or 8192-slot shared table up to 4096 distinct candidates, a
 //     1024-thread block with a 16384-slot shared table above that, and a block
-//     with a global table for the rows that overflow it; weights are summed
-//     exactly (int64 / FP64);
+//     with a global table for the rows that overflow it; on coarse graphs of at
+//     most 8192 vertices the block rows use a table indexed by coarse id
+//     instead; weights are summed exactly (int64 / FP64);
 //  5. a prefix sum of the unique counts gives the coarse row offsets;
 //  6. each row is sorted by column and written out: register ranks (<= 32
 //     entries), chunk ranks (sorted 32-key chunks plus binary searches into the
@@ -345,6 +346,78 @@ __global__ void __launch_bounds__(THREADS) k_contract_block(CArgs<W> a, const i3
         }
         __syncthreads();
         if (threadIdx.x == 0) a.ucount[c] = (i64)wcount;
+        __syncthreads();
+    }
+}
+
+// ---- block rows of small coarse graphs: a dense table ------------------------
+// With at most DENSE_NC coarse vertices the table is indexed by coarse id:
+// values plus a presence bitmap in shared memory (no keys, no probing, no
+// overflow), and the row is written out in ascending column order by a scan
+// of the bitmap.  The launch takes 8 nc + nc / 8 bytes of shared memory
+// instead of the hash tables' 24-192 KB, so more blocks share an SM.
+constexpr i64 DENSE_NC = 8192;
+
+template <class W, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_contract_dense(CArgs<W> a, const i32* list, const i64* d_count, int nc) {
+    using V = typename Traits<W>::V;
+    constexpr int NW = THREADS / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ u32 wsum[NW];
+    V* vals = (V*)smem_raw;
+    u32* pres = (u32*)(smem_raw + sizeof(V) * (size_t)nc);
+    const int nwords = (nc + 31) >> 5;
+    const int l = lane_id(), w = threadIdx.x >> 5, tid = threadIdx.x;
+    const int per = (nwords + THREADS - 1) / THREADS;
+    const int w0 = min(tid * per, nwords), w1 = min(w0 + per, nwords);
+    const i64 count = *d_count;
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        const i32 c = list[x];
+        const i64 q0 = a.P[a.cstart[c]], q1 = a.P[a.cstart[c + 1]];
+        for (int s = tid; s < nc; s += THREADS) vals[s] = V(0);
+        for (int s = tid; s < nwords; s += THREADS) pres[s] = 0u;
+        __syncthreads();
+        for (i64 q = q0 + (i64)w * 32 + l; q - l < q1; q += THREADS) {
+            i32 key;
+            bool keep, leader;
+            const V sv = cchunk_load(a, q, q1, key, keep, leader);
+            if (leader) {
+                cvatomic_add(&vals[key], sv);
+                atomicOr(&pres[key >> 5], 1u << (key & 31));
+            }
+        }
+        __syncthreads();
+        // exclusive prefix of the word popcounts over the threads' word ranges
+        u32 local = 0;
+        for (int q = w0; q < w1; q++) local += (u32)__popc(pres[q]);
+        u32 incl = local;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const u32 t = __shfl_up_sync(FULL, incl, d);
+            if (l >= d) incl += t;
+        }
+        if (l == 31) wsum[w] = incl;
+        __syncthreads();
+        u32 base = 0, tot = 0;
+#pragma unroll
+        for (int q = 0; q < NW; q++) {
+            const u32 v = wsum[q];
+            base += q < w ? v : 0u;
+            tot += v;
+        }
+        u32 pos = base + incl - local;
+        for (int q = w0; q < w1; q++) {
+            u32 bits = pres[q];
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const i32 key = q * 32 + b;
+                a.out_key[q0 + pos] = key;
+                a.out_val[q0 + pos] = vals[key];
+                pos++;
+            }
+        }
+        if (tid == 0) a.ucount[c] = (i64)tot;
         __syncthreads();
     }
 }
@@ -988,14 +1061,35 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     phase.reset();
     phase.emplace(ctx, "contract_hash");
     const size_t slot = sizeof(V) + sizeof(i32);
-    if (n_b > 0) {
+    const bool dense = nc <= DENSE_NC;
+    if (dense && (n_b > 0 || n_b2 > 0 || n_h > 0)) {
+        // every block row on the dense table (256 threads up to U = 1024, 512 above)
+        const size_t dsmem = sizeof(V) * (size_t)nc + sizeof(u32) * (size_t)ceil_div(nc, 32);
+        const int dmax = (int)(sizeof(V) * DENSE_NC + sizeof(u32) * (DENSE_NC / 32));
+        set_dynamic_smem_once(k_contract_dense<W, 256>, dmax, ctx.device);
+        set_dynamic_smem_once(k_contract_dense<W, 512>, dmax, ctx.device);
+        if (n_b > 0) {
+            int grid = (int)std::min<i64>(n_b, (i64)ctx.num_sms * 8);
+            k_contract_dense<W, 256><<<grid, 256, dsmem, ctx.stream>>>(a, lb.p, counts.p + 2, (int)nc);
+            PGGC_LAUNCH_CHECK();
+        }
+        const i64 lists[2] = {n_b2, n_h};
+        const i32* lp[2] = {lb2.p, lh.p};
+        for (int q = 0; q < 2; q++) {
+            if (lists[q] <= 0) continue;
+            int grid = (int)std::min<i64>(lists[q], (i64)ctx.num_sms * 4);
+            k_contract_dense<W, 512><<<grid, 512, dsmem, ctx.stream>>>(a, lp[q], counts.p + 3 + q, (int)nc);
+            PGGC_LAUNCH_CHECK();
+        }
+    }
+    if (!dense && n_b > 0) {
         constexpr int TS = 2048;
         int grid = (int)std::min<i64>(n_b, (i64)ctx.num_sms * 8);
         k_contract_block<W, false, 256><<<grid, 256, slot * TS, ctx.stream>>>(a, lb.p, counts.p + 2, nullptr, nullptr,
                                                                                TS, nc);
         PGGC_LAUNCH_CHECK();
     }
-    if (n_b2 > 0) {
+    if (!dense && n_b2 > 0) {
         constexpr int TS = 2 * HUGE_DEG;
         set_dynamic_smem_once(k_contract_block<W, false, 512>, (int)(slot * TS), ctx.device);
         int grid = (int)std::min<i64>(n_b2, (i64)ctx.num_sms * 2);
@@ -1003,7 +1097,7 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
                                                                                TS, nc);
         PGGC_LAUNCH_CHECK();
     }
-    if (n_h > 0) {
+    if (!dense && n_h > 0) {
         // 16384-slot shared tables; rows with more distinct neighbours (a
         // 64-probe insert failure) go to the overflow list
         constexpr int TS = 16384;
