@@ -75,7 +75,7 @@ SUB_PHASES = ("contract_prep", "contract_hash", "contract_place", "contract_plac
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8, help="timed clustering runs (population members)")
+    ap.add_argument("--steps", type=int, default=12, help="timed clustering runs (population members)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4194304, help="DC-SBM vertex count (default: the named workload)")
@@ -85,7 +85,7 @@ def parse():
                     help="plain runs for the ratio (the first seeds of the population, no filter, one stream; "
                          "-1: every seed of the population, so both arms run the same seeds, stopping after "
                          "--plain-budget seconds once two runs are done)")
-    ap.add_argument("--plain-budget", type=float, default=120.0,
+    ap.add_argument("--plain-budget", type=float, default=200.0,
                     help="wall-clock bound of the plain arm when --plain-runs is -1")
     ap.add_argument("--no-filter", action="store_true", help="batched plain runs (no learned filter)")
     ap.add_argument("--recall", type=float, default=0.995,
