@@ -386,6 +386,104 @@ __global__ void k_hist(i64 n, const i32* lab, i64* cnt) {
         ::atomicAdd((unsigned long long*)&cnt[lab[i]], 1ull);
 }
 
+// The vertices grouped by tree and ordered by (order, id) inside each tree --
+// the order of a stable sort on (tree, order) -- by a counting sort on the
+// tree id (row_map: tree offsets) followed by per-tree sorts of the 64-bit
+// keys (order << 32 | id): a thread per tree up to SEG_SMALL members (an
+// odd-even transposition network in registers), a block per larger tree
+// (bitonic network in shared memory, up to SEG_BIG members); trees above that
+// fall back to a radix sort of all vertices.
+constexpr int SEG_SMALL = 16;
+constexpr int SEG_MID = 1024;
+constexpr int SEG_BIG = 16384;
+
+__global__ void k_seg_scatter(i64 n, const i32* vcmap, i64* cursor, i32* ids) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        const i64 pos = (i64)::atomicAdd((unsigned long long*)&cursor[vcmap[i]], 1ull);
+        ids[pos] = (i32)i;
+    }
+}
+
+__device__ __forceinline__ u64 seg_key(const i32* order, i32 id) {
+    return ((u64)(u32)order[id] << 32) | (u64)(u32)id;
+}
+
+// sorts the sz <= N ids of one tree by (order, id): an odd-even transposition
+// network of N rounds over keys held in registers (padding ~0 sorts last)
+template <int N>
+__device__ __forceinline__ void seg_sort_net(const i32* order, i32* seg, int sz) {
+    u64 k[N];
+#pragma unroll
+    for (int t = 0; t < N; t++) k[t] = t < sz ? seg_key(order, seg[t]) : ~0ull;
+#pragma unroll
+    for (int rd = 0; rd < N; rd++) {
+#pragma unroll
+        for (int t = rd & 1; t + 1 < N; t += 2) {
+            const u64 lo = k[t] < k[t + 1] ? k[t] : k[t + 1];
+            const u64 hi = k[t] < k[t + 1] ? k[t + 1] : k[t];
+            k[t] = lo;
+            k[t + 1] = hi;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < N; t++)
+        if (t < sz) seg[t] = (i32)(u32)k[t];
+}
+
+// trees of 2..SEG_SMALL members sorted in registers; larger ones listed
+// (big[0]: count of trees of up to SEG_MID members, big[1]: up to SEG_BIG,
+// big[2]: above; the lists grow from the two ends of `lst`)
+__global__ void k_seg_sort_small(i64 n, const i64* row_map, const i32* order, i32* ids, i32* lst,
+                                 unsigned long long* big) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < n; r += (i64)gridDim.x * blockDim.x) {
+        const i64 b = row_map[r], sz = row_map[r + 1] - b;
+        if (sz <= 1) continue;
+        if (sz > SEG_SMALL) {
+            if (sz <= SEG_MID) lst[::atomicAdd(&big[0], 1ull)] = (i32)r;
+            else if (sz <= SEG_BIG) lst[n - 1 - (i64)::atomicAdd(&big[1], 1ull)] = (i32)r;
+            else ::atomicAdd(&big[2], 1ull);
+            continue;
+        }
+        if (sz <= 4) seg_sort_net<4>(order, ids + b, (int)sz);
+        else if (sz <= 8) seg_sort_net<8>(order, ids + b, (int)sz);
+        else seg_sort_net<SEG_SMALL>(order, ids + b, (int)sz);
+    }
+}
+
+// a block per listed tree: keys in shared memory, bitonic network over
+// next_pow2(size) slots padded with ~0
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_seg_sort_block(const i32* lst, i64 count, const i64* row_map,
+                                                            const i32* order, i32* ids) {
+    extern __shared__ __align__(16) u64 sk[];
+    for (i64 x = blockIdx.x; x < count; x += gridDim.x) {
+        const i32 r = lst[x];
+        const i64 b = row_map[r];
+        const u32 sz = (u32)(row_map[r + 1] - b);
+        const u32 T = next_pow2_u32(sz);
+        for (u32 s = threadIdx.x; s < T; s += THREADS) sk[s] = s < sz ? seg_key(order, ids[b + s]) : ~0ull;
+        __syncthreads();
+        for (u32 k = 2; k <= T; k <<= 1) {
+            for (u32 j = k >> 1; j > 0; j >>= 1) {
+                for (u32 t = threadIdx.x; t < T; t += THREADS) {
+                    const u32 q = t ^ j;
+                    if (q > t) {
+                        const bool up = (t & k) == 0;
+                        const u64 a0 = sk[t], a1 = sk[q];
+                        if ((a0 > a1) == up) {
+                            sk[t] = a1;
+                            sk[q] = a0;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (u32 s = threadIdx.x; s < sz; s += THREADS) ids[b + s] = (i32)(u32)sk[s];
+        __syncthreads();
+    }
+}
+
 template <class V>
 struct TsIn;
 template <>
@@ -588,7 +686,7 @@ __global__ void k_contig_apply(i64 n, const i32* vcmap, const i32* newid, i32* o
 // through the allocator for them.
 enum RefineSlot : int {
     RS_PV = 90, RS_WELL, RS_HN, RS_ORDER, RS_VCMAP, RS_KEYS, RS_KEYS2, RS_IDS, RS_IDS2, RS_CNT, RS_ROWMAP, RS_TS,
-    RS_INNER, RS_OC, RS_INC, RS_BREAK, RS_NEWID, RS_TOT
+    RS_INNER, RS_OC, RS_INC, RS_BREAK, RS_NEWID, RS_TOT, RS_SEGBIG
 };
 template <class T>
 struct RBuf {
@@ -667,16 +765,45 @@ i64 coarsen_leidenR(Context& ctx, const Graph<W>& g, const Ordering& ord, const 
     PGGC_LAUNCH_CHECK();
 
     // --- gamma connectivity
-    RBuf<u64> keys(ctx, RS_KEYS, n), keys2(ctx, RS_KEYS2, n);
-    RBuf<i32> ids(ctx, RS_IDS, n), ids2(ctx, RS_IDS2, n);
-    k_sort_keys<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, order.p, keys.p, ids.p);
-    PGGC_LAUNCH_CHECK();
-    radix_sort_pairs<i32>(ctx, keys.p, ids.p, n, 0, 31 + bits_for((u64)(n - 1)), keys2.p, ids2.p);
+    // tree offsets, then the vertices grouped by tree in (order, id) order
     RBuf<i64> cnt(ctx, RS_CNT, n + 1), row_map(ctx, RS_ROWMAP, n + 1);
     PGGC_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(i64) * (n + 1), ctx.stream));
     k_hist<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, cnt.p);
     PGGC_LAUNCH_CHECK();
     scan_apply(ctx, ArrIn{cnt.p}, ArrOutExcl{row_map.p}, n + 1, nullptr, nullptr);
+    RBuf<i32> ids(ctx, RS_IDS, n), lst(ctx, RS_IDS2, n);
+    {
+        copy_d2d(ctx, cnt.p, row_map.p, n + 1);  // scatter cursors
+        k_seg_scatter<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, cnt.p, ids.p);
+        PGGC_LAUNCH_CHECK();
+        RBuf<unsigned long long> big(ctx, RS_SEGBIG, 4);
+        PGGC_CUDA(cudaMemsetAsync(big.p, 0, sizeof(unsigned long long) * 4, ctx.stream));
+        k_seg_sort_small<<<grid, 256, 0, ctx.stream>>>(n, row_map.p, order.p, ids.p, lst.p, big.p);
+        PGGC_LAUNCH_CHECK();
+        const unsigned long long* hb = (const unsigned long long*)ctx.readback(big.p, 3 * sizeof(unsigned long long));
+        const i64 n_mid = (i64)hb[0], n_big = (i64)hb[1], n_huge = (i64)hb[2];
+        if (n_huge > 0) {
+            // a tree above SEG_BIG members: the radix sort of every vertex on (tree, order)
+            RBuf<u64> keys(ctx, RS_KEYS, n), keys2(ctx, RS_KEYS2, n);
+            k_sort_keys<<<grid, 256, 0, ctx.stream>>>(n, vcmap.p, order.p, keys.p, ids.p);
+            PGGC_LAUNCH_CHECK();
+            radix_sort_pairs<i32>(ctx, keys.p, ids.p, n, 0, 31 + bits_for((u64)(n - 1)), keys2.p, lst.p);
+        } else {
+            if (n_mid > 0) {
+                const int gm = (int)std::min<i64>(n_mid, (i64)ctx.num_sms * 8);
+                k_seg_sort_block<256><<<gm, 256, sizeof(u64) * SEG_MID, ctx.stream>>>(lst.p, n_mid, row_map.p,
+                                                                                     order.p, ids.p);
+                PGGC_LAUNCH_CHECK();
+            }
+            if (n_big > 0) {
+                set_dynamic_smem_once(k_seg_sort_block<1024>, (int)(sizeof(u64) * SEG_BIG), ctx.device);
+                const int gb2 = (int)std::min<i64>(n_big, (i64)ctx.num_sms);
+                k_seg_sort_block<1024><<<gb2, 1024, sizeof(u64) * SEG_BIG, ctx.stream>>>(lst.p + (n - n_big), n_big,
+                                                                                         row_map.p, order.p, ids.p);
+                PGGC_LAUNCH_CHECK();
+            }
+        }
+    }
     RBuf<V> ts(ctx, RS_TS, n), inner(ctx, RS_INNER, n), oc(ctx, RS_OC, n);
     if constexpr (std::is_same<V, i64>::value) {
         scan_apply(ctx, TsIn<i64>{ids.p, g.vtx_w.p, n}, ArrOutExcl{ts.p}, n, nullptr, nullptr);

@@ -470,3 +470,31 @@ def test_build_coarse_graph_member_layouts(mem, weighted):
         assert rg[1] == rg[0] == 0
         if nc == 40000:
             assert rg[2] - rg[1] > 16384
+
+
+@pytest.mark.parametrize("sizes", [[5000, 500, 30, 10, 3], [20000, 700, 12]])
+def test_coarsen_leidenR_tree_sizes(mem, sizes):
+    """Disjoint stars: the refinement's trees have ~every star's size, so the
+    per-tree sorts run in registers (<= 16 members), per block (<= 1024 and
+    <= 16384) and, with a 20,000-leaf star, fall back to the radix sort of all
+    vertices."""
+    edges, v = [], 0
+    for sz in sizes:
+        c = v
+        edges += [(c, c + 1 + k) for k in range(sz)]
+        v += sz + 1
+    hg = G.from_edges(v, edges)
+    og, wg = _pair(mem, hg, pg.OBJ_MOD)
+    cd_o = O.ClusterData(og, pg.OBJ_MOD, 1.0)
+    cd_g = pg.get_objective(mem, wg, pg.OBJ_MOD, 1.0)
+    part = np.arange(v, dtype=np.int32)
+    po, _, _ = O.local_move(og, cd_o, part, True)
+    pgp = part.copy()
+    pg.local_move(mem, wg, pgp, cd_g, True)
+    assert np.array_equal(po, pgp)
+    for seeds in [(1, 2), (12345, 678)]:
+        vo, nco = O.coarsen_leidenR(og, cd_o, po, *seeds)
+        vg, ncg = pg.coarsen_leidenR(mem, wg, pgp, cd_g, *seeds)
+        assert nco == ncg
+        assert np.array_equal(vo, vg)
+    assert np.bincount(vo).max() >= sizes[0] - 30
