@@ -85,7 +85,7 @@ def parse():
                     help="plain runs for the ratio (the first seeds of the population, no filter, one stream; "
                          "-1: every seed of the population, so both arms run the same seeds, stopping after "
                          "--plain-budget seconds once two runs are done)")
-    ap.add_argument("--plain-budget", type=float, default=200.0,
+    ap.add_argument("--plain-budget", type=float, default=150.0,
                     help="wall-clock bound of the plain arm when --plain-runs is -1")
     ap.add_argument("--no-filter", action="store_true", help="batched plain runs (no learned filter)")
     ap.add_argument("--recall", type=float, default=0.995,
