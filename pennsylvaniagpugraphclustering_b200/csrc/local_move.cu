@@ -1461,6 +1461,34 @@ __global__ void k_mark_affected(DGraph<W> g, const i32* moves, i64 nm, unsigned 
     }
 }
 
+// The same flags pulled instead of pushed: the movers are flagged 2 first
+// (k_mark_movers), then a warp per vertex looks for a flagged-2 neighbour 32
+// edges at a time and stops at the first one.  Pushing costs the movers'
+// degrees, pulling about n / (moved fraction) edges, so dense graphs with
+// many movers pull.  The graph is symmetric, so "has a moved neighbour" is
+// "is a neighbour of a mover": the flagged set is the same.
+__global__ void k_mark_movers(const i32* moves, i64 nm, unsigned char* flags) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < nm; x += (i64)gridDim.x * blockDim.x)
+        flags[moves[x]] = 2;
+}
+
+template <class W>
+__global__ void k_mark_pull(DGraph<W> g, unsigned char* flags) {
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    const int l = lane_id();
+    for (i64 i = gw; i < g.n; i += nw) {
+        if (flags[i] == 2) continue;
+        const i64 b = g.rowptr[i], e = g.rowptr[i + 1];
+        bool hit = false;
+        for (i64 j0 = b; j0 < e && !hit; j0 += 32) {
+            const i64 j = j0 + l;
+            hit = __any_sync(FULL, j < e && flags[g.col[j]] == 2);
+        }
+        if (hit && l == 0) flags[i] = 1;
+    }
+}
+
 // Affected vertices of a sweep (the movers and their neighbours), listed once
 // each: vertices below MASSIVE_CUTOFF go to `list` (first marker of the
 // epoch appends), massive ones are flagged for the block kernel.
@@ -2157,8 +2185,18 @@ struct Mover {
             own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 0, nullptr, nullptr, &cls);
             fill<i32>(ctx, dest.p, n, NULL_PART);
         } else if (nm * 16 > n) {
-            k_mark_affected<W><<<grid_for(ctx, ceil_div(nm, 8), 1, 16), 256, 0, ctx.stream>>>(gv, moves.p, nm, flags.p);
-            PGGC_LAUNCH_CHECK();
+            // push costs nm * avg_deg edges, pull about n * n / nm
+            const double avg_deg = (double)g.nnz / (double)std::max<i64>(n, 1);
+            if ((double)nm * (double)nm * avg_deg > 4.0 * (double)n * (double)n) {
+                k_mark_movers<<<grid_for(ctx, nm, 256), 256, 0, ctx.stream>>>(moves.p, nm, flags.p);
+                PGGC_LAUNCH_CHECK();
+                k_mark_pull<W><<<grid_for(ctx, ceil_div(n, 8), 1, 16), 256, 0, ctx.stream>>>(gv, flags.p);
+                PGGC_LAUNCH_CHECK();
+            } else {
+                k_mark_affected<W><<<grid_for(ctx, ceil_div(nm, 8), 1, 16), 256, 0, ctx.stream>>>(gv, moves.p, nm,
+                                                                                                flags.p);
+                PGGC_LAUNCH_CHECK();
+            }
             own_weights_impl<W>(ctx, g, ord, part.p, pvals.p, 1, flags.p, dest.p, &cls);
         } else {
             // few moves: list the affected vertices once and recompute only them
