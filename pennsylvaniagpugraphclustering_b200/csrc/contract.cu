@@ -112,6 +112,45 @@ __global__ void __launch_bounds__(256) k_flatten(DGraph<W> g, const i32* vcmap, 
     }
 }
 
+// Flattening of graphs with long rows (mean degree >= FLW_MIN_DEG: the dense
+// coarse levels, a few thousand vertices of thousands of edges): a warp per
+// vertex copies its row, 4 chunks of 32 edges in flight, so the work spreads
+// over n warps instead of n / 32.
+constexpr i64 FLW_MIN_DEG = 128;
+
+template <class W>
+__global__ void __launch_bounds__(256) k_flatten_wide(DGraph<W> g, const i32* vcmap, const i64* P,
+                                                      const i64* memberpos, i32* fkey, W* fw) {
+    const int l = lane_id();
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
+    for (i64 u = gw; u < g.n; u += nw) {
+        const i64 b = g.rowptr[u], e = g.rowptr[u + 1];
+        const i64 base = P[memberpos[u]] - b;  // flat position of edge j: base + j
+        const i32 cu = vcmap[u];
+        constexpr int UNR = 4;
+        for (i64 j0 = b; j0 < e; j0 += 32 * UNR) {
+            i32 col[UNR];
+            W wv[UNR];
+#pragma unroll
+            for (int k = 0; k < UNR; k++) {
+                const i64 j = j0 + 32 * k + l;
+                col[k] = j < e ? g.col[j] : 0;
+                wv[k] = (g.w && j < e) ? g.w[j] : W(0);
+            }
+#pragma unroll
+            for (int k = 0; k < UNR; k++) {
+                const i64 j = j0 + 32 * k + l;
+                if (j < e) {
+                    const i32 cv = vcmap[col[k]];
+                    fkey[base + j] = cv == cu ? -1 : cv;
+                    if (g.w) fw[base + j] = wv[k];
+                }
+            }
+        }
+    }
+}
+
 struct MemberDegIn {
     const i64* rowptr;
     const i32* members;
@@ -1001,7 +1040,11 @@ std::unique_ptr<Graph<W>> build_coarse_graph(Context& ctx, const Graph<W>& g, co
     // flattened rows: coarse key and weight of every fine edge at its flat position
     WsBuf<i32> fkey(ctx, CS_FKEY, g.nnz);
     W* fw_p = gv.w ? ctx.ws_get<W>(CS_FW, std::max<i64>(g.nnz, 1)) : nullptr;
-    if (g.nnz > 0) {
+    if (g.nnz > 0 && g.nnz >= FLW_MIN_DEG * n) {
+        int grid = (int)std::min<i64>(ceil_div(n, 8), (i64)ctx.num_sms * 16);
+        k_flatten_wide<W><<<grid, 256, 0, ctx.stream>>>(gv, vcmap, P.p, memberpos.p, fkey.p, fw_p);
+        PGGC_LAUNCH_CHECK();
+    } else if (g.nnz > 0) {
         int grid = (int)std::min<i64>(ceil_div(ceil_div(n, 32), 8), (i64)ctx.num_sms * 16);
         k_flatten<W><<<grid, 256, 0, ctx.stream>>>(gv, vcmap, P.p, memberpos.p, fkey.p, fw_p);
         PGGC_LAUNCH_CHECK();

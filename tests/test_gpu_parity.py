@@ -498,3 +498,29 @@ def test_coarsen_leidenR_tree_sizes(mem, sizes):
         assert nco == ncg
         assert np.array_equal(vo, vg)
     assert np.bincount(vo).max() >= sizes[0] - 30
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_build_coarse_graph_dense_rows(mem, weighted):
+    """A graph with long rows (9,000 vertices, mean degree ~145, the shape of
+    the coarse levels): the warp-per-vertex flattening, with 300 coarse
+    vertices the dense-table hashing and with 9,000 the hash tables."""
+    rng = np.random.default_rng(23)
+    n, m = 9000, 1300000
+    src = rng.integers(0, n, m)
+    dst = rng.integers(0, n, m)
+    keep = src < dst
+    pairs = np.unique(np.stack([src[keep], dst[keep]], axis=1), axis=0)
+    edges = list(map(tuple, pairs.tolist()))
+    w = rng.uniform(0.5, 1.5, len(edges)).astype(np.float32) if weighted else None
+    hg = G.from_edges(n, edges, w)
+    assert hg.nnz >= 128 * n
+    obj = pg.OBJ_WMOD if weighted else pg.OBJ_MOD
+    og, wg = _pair(mem, hg, obj)
+    for nc in (300, 9000):
+        vcmap = rng.integers(0, nc, n).astype(np.int32)
+        vcmap[:nc] = np.arange(nc, dtype=np.int32)
+        co = O.build_coarse_graph(og, vcmap, nc)
+        cg = pg.build_coarse_graph(mem, wg, vcmap, nc)
+        for x, y in zip(co.arrays(), cg.to_host()):
+            assert np.array_equal(x, y)
